@@ -1,0 +1,216 @@
+// Device-side data layout and the per-cell update arithmetic shared by the
+// step kernels. Every expression keeps the evaluation order of the
+// reference OpenCL kernels it restates; the engine is compiled with
+// -fmad=false so no multiply-add contraction changes a rounding, which makes
+// the FP32 results reproducible operation by operation on the CPU.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace afd {
+
+// Field layout of one batch member: x-fastest rows padded to `pitch`
+// floats, index = z*plane + y*pitch + x.
+struct GridDev {
+    int32_t nx, ny, nz;
+    int64_t pitch, plane, vol;
+};
+
+// Compact boundary (LRS) list. Entry e: linear cell index, packed info
+// (group | mat0 << 5 | mat1 << 13 | mat2 << 21) and filter state
+// st_in/st_out[(b*S + slot)*n + e], S = 3*K slots per entry.
+struct LrsDev {
+    int32_t n;
+    int32_t K, S;
+    const int32_t* cell;
+    const uint32_t* info;
+    float* st_in;
+    float* st_out;
+    const float* ca;  // [nmat][K]
+    const float* cb;  // [nmat][K]
+    float l, l2, c2;  // coefficient l, l*l and 2(1-3*l*l)
+};
+
+// PML state. Full-grid auxiliary fields (two time levels each) per batch
+// member; ksi profiles padded with zeros to kmax entries.
+struct PmlDev {
+    int32_t width;     // 0: PML off
+    uint32_t faces;    // FIXED-mode face mask
+    int64_t g0;        // global step at which the PML was enabled
+    float* fi[3][2];   // [axis][level]
+    float* psi[2];
+    const float* ksi[3];
+    // FIXED mode: compact list of PML cells with slab flags (bit a = axis a)
+    int32_t n_cells;
+    const int32_t* cells;
+    const uint8_t* flags;
+    // scalars, each computed on the host in FP32 exactly as the reference
+    // kernel expression would compute it (pml.cl:185-262)
+    float dt, cc_dxdx, inv_dx, half_inv_dx, inv_dt2, two_dt, inv_dt;
+};
+
+struct SrcDev {
+    int32_t n;
+    const int32_t* cell;
+    const int32_t* begin;   // [batch+1] range of sources of each member
+    const int64_t* off;
+    const int64_t* len;
+    const float* data;
+};
+
+struct RcvDev {
+    int32_t n;
+    const int32_t* cell;
+    float* out;      // [batch][n][cap]
+    int64_t cap;
+};
+
+struct StepArgs {
+    GridDev g;
+    int32_t batch;
+    int32_t mode;             // AFD_MODE_REF / AFD_MODE_FIXED
+    float* p[3];              // three rotating field buffers, each [batch][vol]
+    const long long* d_step;  // global step index at the start of the chunk
+    float lambda2, cint;      // interior: lambda^2 and 2(1-3 lambda^2)
+    LrsDev lrs;
+    PmlDev pml;
+    SrcDev src;
+    RcvDev rcv;
+    int* flag;                // watchdog flag (bit0: |p| left the bound)
+};
+
+// Buffer roles of global step g, following the pointer rotation of
+// simulation.hpp:360 (three buffers rotated right by one per step):
+// the new level is written into buffer (2 + 2g) mod 3.
+__host__ __device__ inline int buf_new(long long g) { return (int)((2 + 2 * (g % 3)) % 3); }
+__host__ __device__ inline int buf_cur(long long g) { return (buf_new(g) + 1) % 3; }
+__host__ __device__ inline int buf_old(long long g) { return (buf_new(g) + 2) % 3; }
+
+// Ring slot written at global step g (simulation.hpp:365: decremented
+// before every step, starting from 0).
+__host__ __device__ inline int ring_index(long long g, int K) { return K - 1 - (int)(g % K); }
+
+// Interior SLF update, leapfrog.cl:41-53.
+__device__ __forceinline__ float slf_update(float lambda2, float cint, float xp, float xm, float yp,
+                                            float ym, float zp, float zm, float c, float old) {
+    float s = xp + xm;
+    s = s + yp;
+    s = s + ym;
+    s = s + zp;
+    s = s + zm;
+    return lambda2 * s + cint * c - old;
+}
+
+// Neighbour sum of a boundary cell: axes in x, y, z order; a wall on the +
+// side contributes 2*p(-1), on the - side 2*p(+1), none p(+1) + p(-1)
+// (lrs_1.cl:80-120, lrs_2.cl:89-207, lrs_3.cl:96-174).
+__device__ __forceinline__ float lrs_neighbour_sum(unsigned mask, const float nb[6]) {
+    // nb: p at x+1, x-1, y+1, y-1, z+1, z-1
+    float s;
+    bool first = true;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        float t0, t1;
+        int n;
+        if (mask & (1u << (2 * ax))) {          // wall on the + side
+            t0 = 2.0f * nb[2 * ax + 1];
+            n = 1;
+        } else if (mask & (1u << (2 * ax + 1))) {  // wall on the - side
+            t0 = 2.0f * nb[2 * ax];
+            n = 1;
+        } else {
+            t0 = nb[2 * ax];
+            t1 = nb[2 * ax + 1];
+            n = 2;
+        }
+        if (first) {
+            s = t0;
+            first = false;
+        } else {
+            s = s + t0;
+        }
+        if (n == 2) s = s + t1;
+    }
+    return s;
+}
+
+__constant__ uint8_t c_group_mask[26];
+
+// One boundary point update. Returns p^{n+1} of the cell and writes the
+// filter state of every face. `pint` is the interior (leapfrog) value of
+// the cell, kept by the corner group that the reference never updates
+// (group 25 in REF mode). `pc`, `pold`: p^n and p^{n-1} of the cell.
+// REF semantics: lrs_1.cl:61-124, lrs_2.cl:61-215, lrs_3.cl:61-186 with the
+// host call of simulation.hpp:368-369. FIXED: l is the Courant number,
+// corners use all three filters with a ring of K slots each, group 25 is a
+// regular corner.
+template <bool REF>
+__device__ __forceinline__ float lrs_point(const LrsDev& L, int e, int b, uint32_t info,
+                                           const float nb[6], float pc, float pold, float pint,
+                                           int ix_buf) {
+    const int group = (int)(info & 31u);
+    const int nf = group < 6 ? 1 : (group < 18 ? 2 : 3);
+    const int K = L.K;
+    int mat[3] = {(int)((info >> 5) & 255u), (int)((info >> 13) & 255u), (int)((info >> 21) & 255u)};
+    // ring width per filter: K, except REF corners (lrs_3.cl:70, size_a_0/2)
+    const int size_f = (REF && nf == 3) ? K / 2 : K;
+    const size_t n = (size_t)L.n;
+    float* sin_ = L.st_in + (size_t)b * L.S * n + e;
+    float* sout = L.st_out + (size_t)b * L.S * n + e;
+
+    float a0[3], b0[3], gn[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        gn[f] = 0.0f;
+        a0[f] = 1.0f;
+        b0[f] = 1.0f;
+        if (f < nf) {
+            a0[f] = __ldg(L.ca + mat[f] * K);
+            b0[f] = __ldg(L.cb + mat[f] * K);
+        }
+    }
+    for (int i = 1; i < K; ++i) {
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            if (f < nf) {
+                const int slot = (ix_buf + i) % size_f + f * size_f;
+                const float bi = __ldg(L.cb + mat[f] * K + i);
+                const float ai = __ldg(L.ca + mat[f] * K + i);
+                gn[f] += bi * sin_[(size_t)slot * n] - ai * sout[(size_t)slot * n];
+            }
+        }
+    }
+
+    const float l = L.l, l2 = L.l2;
+    const float S = lrs_neighbour_sum(c_group_mask[group], nb);
+    float pn;
+    if (nf == 1) {
+        pn = (l2 * S + L.c2 * pc + l2 / b0[0] * gn[0] + (l * a0[0] / b0[0] - 1.0f) * pold) /
+             (1.0f + l * a0[0] / b0[0]);
+    } else if (nf == 2 || REF) {
+        if (REF && group == 25) {
+            pn = pint;  // no variant define reaches lrs_3.cl for this group
+        } else {
+            pn = (l2 * S + l2 * (gn[0] / b0[0] + gn[1] / b0[1]) + L.c2 * pc +
+                  (l * a0[0] / b0[0] + l * a0[1] / b0[1] - 1.0f) * pold) /
+                 (1.0f + l * a0[0] / b0[0] + l * a0[1] / b0[1]);
+        }
+    } else {
+        pn = (l2 * S + l2 * (gn[0] / b0[0] + gn[1] / b0[1] + gn[2] / b0[2]) + L.c2 * pc +
+              (l * a0[0] / b0[0] + l * a0[1] / b0[1] + l * a0[2] / b0[2] - 1.0f) * pold) /
+             (1.0f + l * a0[0] / b0[0] + l * a0[1] / b0[1] + l * a0[2] / b0[2]);
+    }
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        if (f < nf) {
+            const float xn = a0[f] / (l * b0[f]) * (pn - pold) - gn[f] / b0[f];
+            const int slot = ix_buf + f * size_f;
+            sin_[(size_t)slot * n] = xn;
+            sout[(size_t)slot * n] = 1.0f / a0[f] * (b0[f] * xn + gn[f]);
+        }
+    }
+    return pn;
+}
+
+}  // namespace afd

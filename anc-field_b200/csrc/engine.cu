@@ -1,0 +1,1238 @@
+// Simulation engine: device memory, compact lists, step kernels and the
+// chunked step loop (per-step launches or replayed CUDA graphs).
+//
+// Per time step (simulation.hpp:358-393) the reference runs leapfrog, 26
+// LRS groups, the PML kernel, source and mic. Here a step is either
+//   fused:   one step kernel (interior + boundary + FIXED-mode PML pressure +
+//            source + receiver) and, with a FIXED-mode PML, one kernel for
+//            the auxiliary PML fields;
+//   unfused: interior, boundary, PML and source/receiver kernels in turn.
+// REF mode with a PML always takes the unfused order, because the
+// reference PML kernel reads the boundary-updated pressure of its
+// neighbours (pml.cl:124-137).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+#include "engine.hpp"
+
+namespace afd {
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t err__ = (call);                                                     \
+        if (err__ != cudaSuccess)                                                       \
+            throw Error(AFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(err__)); \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T* ptr = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        release();
+        if (count == 0) return;
+        CK(cudaMalloc(&ptr, count * sizeof(T)));
+        n = count;
+        CK(cudaMemset(ptr, 0, count * sizeof(T)));
+    }
+    void upload(const std::vector<T>& v) {
+        alloc(v.size());
+        if (!v.empty()) CK(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Unfused kernels (one launch per sub-step, the reference's order)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void watch(int* flag, float v) {
+    if (!(fabsf(v) < 1e30f)) atomicOr(flag, 1);
+}
+
+// leapfrog.cl:34-55 over 1 <= x,y,z <= n-2 of every batch member.
+__global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int zn = a.g.nz - 2;
+    const int b = blockIdx.z / zn;
+    const int z = 1 + blockIdx.z % zn;
+    if (x > a.g.nx - 2 || y > a.g.ny - 2) return;
+    const size_t base = (size_t)b * a.g.vol;
+    float* pn = a.p[buf_new(g)] + base;
+    const float* pc = a.p[buf_cur(g)] + base;
+    const float* po = a.p[buf_old(g)] + base;
+    const int64_t i = (int64_t)z * a.g.plane + (int64_t)y * a.g.pitch + x;
+    const float v = slf_update(a.lambda2, a.cint, pc[i + 1], pc[i - 1], pc[i + a.g.pitch],
+                               pc[i - a.g.pitch], pc[i + a.g.plane], pc[i - a.g.plane], pc[i], po[i]);
+    pn[i] = v;
+    watch(a.flag, v);
+}
+
+// The 26 lrs_k launches of simulation.hpp:366-370 as one launch over the
+// compact list.
+template <bool REF>
+__global__ void __launch_bounds__(256) k_lrs(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.lrs.n) return;
+    const int b = blockIdx.y;
+    const size_t base = (size_t)b * a.g.vol;
+    float* pn = a.p[buf_new(g)] + base;
+    const float* pc = a.p[buf_cur(g)] + base;
+    const float* po = a.p[buf_old(g)] + base;
+    const int64_t c = a.lrs.cell[e];
+    const uint32_t info = a.lrs.info[e];
+    const float nb[6] = {pc[c + 1], pc[c - 1], pc[c + a.g.pitch], pc[c - a.g.pitch],
+                         pc[c + a.g.plane], pc[c - a.g.plane]};
+    const float v = lrs_point<REF>(a.lrs, e, b, info, nb, pc[c], po[c], pn[c],
+                                   ring_index(g, a.lrs.K));
+    pn[c] = v;
+}
+
+// ---- PML -------------------------------------------------------------------
+// Face averages of pml.cl:74-122 (fi_*_avg, p_*_avg, psi_*_avg share one
+// pattern each): x-faces average over (y, y+1) x (z, z+1), y-faces over
+// (x, x+1) x (z, z+1), z-faces over (x, x+1) x (y, y+1). `own` replaces the
+// value of cell `self` when it is one of the four (the reference kernel's
+// own write becomes visible to its later reads, pml.cl:185-188).
+struct Avg {
+    const float* f;
+    int64_t self;
+    float own;
+    bool subst;
+    __device__ __forceinline__ float v(int64_t i) const { return (subst && i == self) ? own : f[i]; }
+    __device__ __forceinline__ float ax(int64_t i, int64_t pitch, int64_t plane) const {
+        return 0.25f * (((v(i) + v(i + plane)) + v(i + pitch)) + v(i + pitch + plane));
+    }
+    __device__ __forceinline__ float ay(int64_t i, int64_t pitch, int64_t plane) const {
+        return 0.25f * (((v(i) + v(i + plane)) + v(i + 1)) + v(i + 1 + plane));
+    }
+    __device__ __forceinline__ float az(int64_t i, int64_t pitch, int64_t plane) const {
+        return 0.25f * (((v(i) + v(i + pitch)) + v(i + 1)) + v(i + 1 + pitch));
+    }
+};
+
+// PML pressure update, pml.cl:185-207. Returns p^{n+1}; psi_new receives
+// psi^{n+1/2} = dt*p^n + psi^{n-1/2}.
+__device__ __forceinline__ float pml_pressure(const StepArgs& a, const float* pc, const float* po,
+                                              const float* fx1, const float* fy1, const float* fz1,
+                                              const float* psimh, int x, int y, int z, int64_t i,
+                                              float* psi_new) {
+    const PmlDev& P = a.pml;
+    const int64_t pitch = a.g.pitch, plane = a.g.plane;
+    const float kx = P.ksi[0][x], ky = P.ksi[1][y], kz = P.ksi[2][z];
+    const float pm1 = pc[i];
+    const float ps = P.dt * pm1 + psimh[i];
+    *psi_new = ps;
+    float s = pc[i + 1] + pc[i - 1];
+    s = s + pc[i + pitch];
+    s = s + pc[i - pitch];
+    s = s + pc[i + plane];
+    s = s + pc[i - plane];
+    s = s - 6.0f * pm1;
+    const float A = P.cc_dxdx * s;
+    const Avg FX{fx1, -1, 0.0f, false}, FY{fy1, -1, 0.0f, false}, FZ{fz1, -1, 0.0f, false};
+    float d = FX.ax(i + 1, pitch, plane) - FX.ax(i, pitch, plane);
+    d = d + FY.ay(i + pitch, pitch, plane);
+    d = d - FY.ay(i, pitch, plane);
+    d = d + FZ.az(i + plane, pitch, plane);
+    d = d - FZ.az(i, pitch, plane);
+    const float B = P.inv_dx * d;
+    const float C = kx * ky * kz * 0.5f * (ps + psimh[i]);
+    const float D = P.inv_dt2 * (po[i] - 2.0f * pm1);
+    const float E = (kx * ky + ky * kz + kz * kx) * pm1;
+    const float F = (kx + ky + kz) / P.two_dt * po[i];
+    const float num = A + B - C - D - E + F;
+    return num / (P.inv_dt2 + (kx + ky + kz) / P.two_dt);
+}
+
+// Auxiliary field updates of pml.cl:231-262 for one cell. REF: `p` reads
+// see the cell's own new pressure and the other cells' values before the
+// PML pass; the x-derivative's last term reads p (pml.cl:126) and fi_y's
+// psi coefficient reads ksi_x at y (pml.cl:247). FIXED: both corrected.
+template <bool REF>
+__device__ __forceinline__ void pml_aux(const StepArgs& a, unsigned axes, const float* pnew,
+                                        const float* pc, const float* psiph, float p_own,
+                                        float psi_own, const float* fx1, const float* fy1,
+                                        const float* fz1, float* fx, float* fy, float* fz, int x,
+                                        int y, int z, int64_t i) {
+    const PmlDev& P = a.pml;
+    const int64_t pitch = a.g.pitch, plane = a.g.plane;
+    const Avg Pn{pnew, i, p_own, REF}, Pm{pc, -1, 0.0f, false}, Ps{psiph, i, psi_own, REF};
+    const Avg& Plast = REF ? Pn : Pm;
+    const float kax = 0.5f * (P.ksi[0][x] + P.ksi[0][x + 1]);
+    const float kay = 0.5f * (P.ksi[1][y] + P.ksi[1][y + 1]);
+    const float kaz = 0.5f * (P.ksi[2][z] + P.ksi[2][z + 1]);
+    if (axes & 1u) {
+        const float dxp = P.half_inv_dx * (Pn.ax(i + 1, pitch, plane) - Pn.ax(i, pitch, plane) +
+                                           Pm.ax(i + 1, pitch, plane) - Plast.ax(i, pitch, plane));
+        const float dxpsi = P.inv_dx * (Ps.ax(i + 1, pitch, plane) - Ps.ax(i, pitch, plane));
+        const float f1 = fx1[i];
+        fx[i] = (-0.5f * kax * f1 + (kay + kaz - kax) * dxp + (kay * kaz) * dxpsi + P.inv_dt * f1) /
+                (P.inv_dt + kax * 0.5f);
+    }
+    if (axes & 2u) {
+        const float dyp = P.half_inv_dx * (Pn.ay(i + pitch, pitch, plane) - Pn.ay(i, pitch, plane) +
+                                           Pm.ay(i + pitch, pitch, plane) - Plast.ay(i, pitch, plane));
+        const float dypsi = P.inv_dx * (Ps.ay(i + pitch, pitch, plane) - Ps.ay(i, pitch, plane));
+        const float kx_coef = REF ? 0.5f * (P.ksi[0][y] + P.ksi[0][y + 1]) : kax;
+        const float f1 = fy1[i];
+        fy[i] = (-0.5f * kay * f1 + (kax + kaz - kay) * dyp + (kx_coef * kaz) * dypsi + P.inv_dt * f1) /
+                (P.inv_dt + kay * 0.5f);
+    }
+    if (axes & 4u) {
+        const float dzp = P.half_inv_dx * (Pn.az(i + plane, pitch, plane) - Pn.az(i, pitch, plane) +
+                                           Pm.az(i + plane, pitch, plane) - Plast.az(i, pitch, plane));
+        const float dzpsi = P.inv_dx * (Ps.az(i + plane, pitch, plane) - Ps.az(i, pitch, plane));
+        const float f1 = fz1[i];
+        fz[i] = (-0.5f * kaz * f1 + (kax + kay - kaz) * dzp + (kax * kay) * dzpsi + P.inv_dt * f1) /
+                (P.inv_dt + kaz * 0.5f);
+    }
+}
+
+__device__ __forceinline__ int pml_level(const StepArgs& a, long long g) {
+    return (int)((g - a.pml.g0 + 1) & 1);
+}
+
+// REF pass 1: auxiliary fields of every cell 2..n-3, using the cell's own
+// new pressure and psi recomputed locally (nothing written that is read).
+__global__ void __launch_bounds__(256) k_pml_ref_aux(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int x = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int zn = a.g.nz - 4;
+    const int b = blockIdx.z / zn;
+    const int z = 2 + blockIdx.z % zn;
+    if (x > a.g.nx - 3 || y > a.g.ny - 3) return;
+    const int W = a.pml.width;
+    unsigned axes = 0;
+    if (x < W || x > a.g.nx - W - 1) axes |= 1u;
+    if (y < W || y > a.g.ny - W - 1) axes |= 2u;
+    if (z < W || z > a.g.nz - W - 1) axes |= 4u;
+    if (!axes) return;
+    const size_t base = (size_t)b * a.g.vol;
+    const float* pn = a.p[buf_new(g)] + base;
+    const float* pc = a.p[buf_cur(g)] + base;
+    const float* po = a.p[buf_old(g)] + base;
+    const int lv = pml_level(a, g);
+    const float* fx1 = a.pml.fi[0][lv ^ 1] + base;
+    const float* fy1 = a.pml.fi[1][lv ^ 1] + base;
+    const float* fz1 = a.pml.fi[2][lv ^ 1] + base;
+    const float* psiph = a.pml.psi[lv] + base;
+    const float* psimh = a.pml.psi[lv ^ 1] + base;
+    const int64_t i = (int64_t)z * a.g.plane + (int64_t)y * a.g.pitch + x;
+    float psi_new;
+    const float p_new = pml_pressure(a, pc, po, fx1, fy1, fz1, psimh, x, y, z, i, &psi_new);
+    pml_aux<true>(a, axes, pn, pc, psiph, p_new, psi_new, fx1, fy1, fz1, a.pml.fi[0][lv] + base,
+                  a.pml.fi[1][lv] + base, a.pml.fi[2][lv] + base, x, y, z, i);
+}
+
+// REF pass 2: pressure and psi of every cell 2..n-3 (pml.cl:182-207).
+__global__ void __launch_bounds__(256) k_pml_ref_p(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int x = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int zn = a.g.nz - 4;
+    const int b = blockIdx.z / zn;
+    const int z = 2 + blockIdx.z % zn;
+    if (x > a.g.nx - 3 || y > a.g.ny - 3) return;
+    const size_t base = (size_t)b * a.g.vol;
+    float* pn = a.p[buf_new(g)] + base;
+    const float* pc = a.p[buf_cur(g)] + base;
+    const float* po = a.p[buf_old(g)] + base;
+    const int lv = pml_level(a, g);
+    const int64_t i = (int64_t)z * a.g.plane + (int64_t)y * a.g.pitch + x;
+    float psi_new;
+    const float v = pml_pressure(a, pc, po, a.pml.fi[0][lv ^ 1] + base, a.pml.fi[1][lv ^ 1] + base,
+                                 a.pml.fi[2][lv ^ 1] + base, a.pml.psi[lv ^ 1] + base, x, y, z, i,
+                                 &psi_new);
+    a.pml.psi[lv][base + i] = psi_new;
+    pn[i] = v;
+}
+
+// FIXED pass 1 (unfused order): pressure and psi of the PML cells.
+__global__ void __launch_bounds__(256) k_pml_fix_p(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.pml.n_cells) return;
+    const int b = blockIdx.y;
+    const size_t base = (size_t)b * a.g.vol;
+    float* pn = a.p[buf_new(g)] + base;
+    const float* pc = a.p[buf_cur(g)] + base;
+    const float* po = a.p[buf_old(g)] + base;
+    const int lv = pml_level(a, g);
+    const int64_t i = a.pml.cells[e];
+    const int z = (int)(i / a.g.plane);
+    const int y = (int)((i % a.g.plane) / a.g.pitch);
+    const int x = (int)(i % a.g.pitch);
+    float psi_new;
+    const float v = pml_pressure(a, pc, po, a.pml.fi[0][lv ^ 1] + base, a.pml.fi[1][lv ^ 1] + base,
+                                 a.pml.fi[2][lv ^ 1] + base, a.pml.psi[lv ^ 1] + base, x, y, z, i,
+                                 &psi_new);
+    a.pml.psi[lv][base + i] = psi_new;
+    pn[i] = v;
+    watch(a.flag, v);
+}
+
+// FIXED pass 2: auxiliary fields from the complete new pressure and psi.
+__global__ void __launch_bounds__(256) k_pml_fix_aux(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.pml.n_cells) return;
+    const unsigned axes = a.pml.flags[e];
+    if (!axes) return;
+    const int b = blockIdx.y;
+    const size_t base = (size_t)b * a.g.vol;
+    const float* pn = a.p[buf_new(g)] + base;
+    const float* pc = a.p[buf_cur(g)] + base;
+    const int lv = pml_level(a, g);
+    const int64_t i = a.pml.cells[e];
+    const int z = (int)(i / a.g.plane);
+    const int y = (int)((i % a.g.plane) / a.g.pitch);
+    const int x = (int)(i % a.g.pitch);
+    pml_aux<false>(a, axes, pn, pc, a.pml.psi[lv] + base, 0.0f, 0.0f, a.pml.fi[0][lv ^ 1] + base,
+                   a.pml.fi[1][lv ^ 1] + base, a.pml.fi[2][lv ^ 1] + base, a.pml.fi[0][lv] + base,
+                   a.pml.fi[1][lv] + base, a.pml.fi[2][lv] + base, x, y, z, i);
+}
+
+// source.cl:32-40 then mic.cl:32-41 for one batch member per block.
+// Sources landing on one cell are added in insertion order.
+__global__ void k_src_rcv(StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const int b = blockIdx.x;
+    float* pn = a.p[buf_new(g)] + (size_t)b * a.g.vol;
+    if (threadIdx.x == 0) {
+        for (int s = a.src.begin[b]; s < a.src.begin[b + 1]; ++s) {
+            const float v = (g < a.src.len[s]) ? a.src.data[a.src.off[s] + g] : 0.0f;
+            pn[a.src.cell[s]] += v;
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < a.rcv.n; r += blockDim.x) {
+        const float v = pn[a.rcv.cell[r]];
+        a.rcv.out[((size_t)b * a.rcv.n + r) * a.rcv.cap + g] = v;
+        watch(a.flag, v);
+    }
+}
+
+__global__ void k_advance(long long* d_step, int n) { *d_step += n; }
+
+// Discrete SLF energy between the two latest levels u1 (newest) and u0,
+// in FP64: 1/2 sum (u1-u0)^2 + lambda2/2 sum over grid edges of
+// (u1_i-u1_j)(u0_i-u0_j), over the cells 1..n-2 and their edges (edges to
+// the fixed outer faces included once).
+__global__ void k_energy(const float* u1, const float* u0, GridDev g, double lambda2, double* out) {
+    const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = 1 + blockIdx.z;
+    double acc = 0.0;
+    if (x <= g.nx - 2 && y <= g.ny - 2) {
+        const int64_t i = (int64_t)z * g.plane + (int64_t)y * g.pitch + x;
+        const double d = (double)u1[i] - (double)u0[i];
+        acc = 0.5 * d * d;
+        const int64_t off[3] = {1, g.pitch, g.plane};
+        const int lo[3] = {x, y, z};
+        double pot = 0.0;
+        for (int ax = 0; ax < 3; ++ax) {
+            const int64_t jp = i + off[ax];
+            pot += ((double)u1[i] - (double)u1[jp]) * ((double)u0[i] - (double)u0[jp]);
+            if (lo[ax] == 1) {
+                const int64_t jm = i - off[ax];
+                pot += ((double)u1[i] - (double)u1[jm]) * ((double)u0[i] - (double)u0[jm]);
+            }
+        }
+        acc += 0.5 * lambda2 * pot;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// ---------------------------------------------------------------------------
+// Engine implementation
+// ---------------------------------------------------------------------------
+namespace {
+
+void check_cell(const int32_t ijk[3], int32_t nx, int32_t ny, int32_t nz, const char* what) {
+    if (ijk[0] < 0 || ijk[0] >= nx || ijk[1] < 0 || ijk[1] >= ny || ijk[2] < 0 || ijk[2] >= nz) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf, "%s cell (%d,%d,%d) lies outside the %dx%dx%d grid", what,
+                      ijk[0], ijk[1], ijk[2], nx, ny, nz);
+        throw Error(AFD_ERR_ARG, buf);
+    }
+}
+
+}  // namespace
+
+struct Source {
+    int32_t batch;
+    int32_t ijk[3];
+    std::vector<float> sig;
+};
+
+struct Engine::Impl {
+    afd_params prm{};
+    // geometry
+    bool have_model = false;
+    Model model;
+    std::vector<BoundaryPoint> boundary;
+    int32_t min_size[3] = {0, 0, 0};
+    int32_t nx = 0, ny = 0, nz = 0;
+    int64_t pitch = 0, plane = 0, vol = 0;
+    bool initialized = false;
+    int64_t group_counts[kNumGroups] = {};
+    // PML configuration (applied at the next run)
+    int32_t pml_width = 0;
+    uint32_t pml_faces = 0;
+    std::vector<float> ksi[3];
+    bool pml_dirty = false;
+    int64_t pml_g0 = 0;
+    // sources / receivers
+    std::vector<Source> sources;
+    std::vector<std::array<int32_t, 3>> receivers;
+    bool src_dirty = true;
+    int64_t steps_done = 0;
+
+    // device state
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    DBuf<float> fields;  // 3 * batch * vol
+    DBuf<int32_t> lrs_cell;
+    DBuf<uint32_t> lrs_info;
+    DBuf<float> lrs_in, lrs_out;
+    DBuf<float> coef_a, coef_b;
+    DBuf<float> fi[3][2], psi[2];
+    DBuf<float> ksi_dev[3];
+    DBuf<int32_t> pml_cells;
+    DBuf<uint8_t> pml_flags;
+    int64_t n_pml_cells = 0;
+    DBuf<int32_t> src_cell, src_begin;
+    DBuf<int64_t> src_off, src_len;
+    DBuf<float> src_data;
+    DBuf<int32_t> rcv_cell;
+    DBuf<float> rcv_out;
+    int64_t rcv_cap = 0;
+    int32_t rcv_n_dev = 0;
+    DBuf<long long> d_step;
+    DBuf<int> d_flag;
+    DBuf<double> d_energy;
+
+    StepArgs args{};
+    std::map<int64_t, cudaGraphExec_t> graphs;
+    double last_ms = 0.0;
+    int64_t launches = 0;
+    std::vector<KernelStat> kstats;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    std::vector<int> ev_kind;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    bool ref() const { return prm.mode == AFD_MODE_REF; }
+    float lambda2() const {
+        const float t = prm.dt * prm.c / prm.dx;
+        return t * t;
+    }
+    void drop_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+    void grid_dims(int32_t dims[3]) const {
+        if (initialized) {
+            dims[0] = nx;
+            dims[1] = ny;
+            dims[2] = nz;
+            return;
+        }
+        const int32_t md[3] = {have_model ? model.nx : 0, have_model ? model.ny : 0,
+                               have_model ? model.nz : 0};
+        for (int k = 0; k < 3; ++k) dims[k] = std::max(md[k], min_size[k]);
+    }
+
+    void init_device();
+    void setup_pml();
+    void upload_sources();
+    void ensure_receivers(int64_t t_end);
+    void build_args();
+    void launch_step(int j, bool profile);
+    int64_t kernels_per_step() const;
+    void launch_step_count_only(int64_t n) { launches += kernels_per_step() * n + 1; }
+    cudaGraphExec_t graph_for(int64_t n);
+    void run_chunk(int64_t n);
+    void collect_profile();
+};
+
+// Simulation::Init (simulation.hpp:201-231) plus the device copy of
+// LrsData (lrs-data.hpp:116-215): fixes the grid, allocates the three
+// pressure levels and uploads the compact boundary list.
+void Engine::Impl::init_device() {
+    int32_t dims[3];
+    grid_dims(dims);
+    if (dims[0] < 3 || dims[1] < 3 || dims[2] < 3)
+        throw Error(AFD_ERR_STATE, "no grid: load a model or set minsize before run");
+    nx = dims[0];
+    ny = dims[1];
+    nz = dims[2];
+    pitch = ((int64_t)nx + 31) / 32 * 32;
+    plane = pitch * ny;
+    vol = plane * nz;
+    if (vol * 3 > (int64_t)1 << 31 && vol > ((int64_t)1 << 31) - 1)
+        throw Error(AFD_ERR_ARG, "grid too large for 32-bit cell indices");
+    CK(cudaSetDevice(device));
+    fields.alloc((size_t)vol * 3 * prm.batch);
+
+    // boundary list (in the reference's scan order)
+    std::vector<int32_t> cell;
+    std::vector<uint32_t> info;
+    std::fill(group_counts, group_counts + kNumGroups, 0);
+    for (const BoundaryPoint& b : boundary) {
+        cell.push_back((int32_t)(b.z * plane + b.y * pitch + b.x));
+        uint32_t w = (uint32_t)b.group;
+        for (int f = 0; f < 3; ++f)
+            if (b.mat[f] >= 0) w |= (uint32_t)b.mat[f] << (5 + 8 * f);
+        info.push_back(w);
+        group_counts[b.group]++;
+    }
+    lrs_cell.upload(cell);
+    lrs_info.upload(info);
+    const int K = have_model ? model.ncoef : 1;
+    const size_t S = 3 * (size_t)K;
+    lrs_in.alloc(cell.size() * S * prm.batch);
+    lrs_out.alloc(cell.size() * S * prm.batch);
+    if (have_model) {
+        coef_a.upload(model.a);
+        coef_b.upload(model.b);
+    }
+    initialized = true;
+}
+
+// SetPml (simulation.hpp:233-277) applied on the device: fresh auxiliary
+// fields, ksi profiles and, in FIXED mode, the PML cell list.
+void Engine::Impl::setup_pml() {
+    for (int a = 0; a < 3; ++a) {
+        fi[a][0].release();
+        fi[a][1].release();
+        ksi_dev[a].release();
+    }
+    psi[0].release();
+    psi[1].release();
+    pml_cells.release();
+    pml_flags.release();
+    n_pml_cells = 0;
+    pml_g0 = steps_done;
+    pml_dirty = false;
+    if (pml_width <= 0) return;
+    for (int a = 0; a < 3; ++a)
+        for (int l = 0; l < 2; ++l) fi[a][l].alloc((size_t)vol * prm.batch);
+    psi[0].alloc((size_t)vol * prm.batch);
+    psi[1].alloc((size_t)vol * prm.batch);
+    // padded so that the reference's ksi_x[y] read (pml.cl:247) stays in bounds
+    const int32_t kmax = std::max(nx, std::max(ny, nz)) + 1;
+    const int32_t dims[3] = {nx, ny, nz};
+    for (int a = 0; a < 3; ++a) {
+        std::vector<float> k((size_t)kmax, 0.0f);
+        for (int32_t i = 0; i < dims[a] && i < (int32_t)ksi[a].size(); ++i) k[(size_t)i] = ksi[a][(size_t)i];
+        ksi_dev[a].upload(k);
+    }
+    if (!ref()) {
+        // FIXED: non-boundary air cells 2..n-3 inside an enabled face slab
+        std::vector<uint8_t> is_lrs((size_t)nx * ny * nz, 0);
+        for (const BoundaryPoint& b : boundary) is_lrs[((size_t)b.z * ny + b.y) * nx + b.x] = 1;
+        const int W = pml_width;
+        std::vector<int32_t> cells;
+        std::vector<uint8_t> flags;
+        for (int z = 2; z <= nz - 3; ++z)
+            for (int y = 2; y <= ny - 3; ++y)
+                for (int x = 2; x <= nx - 3; ++x) {
+                    unsigned ax = 0;
+                    if (((pml_faces & AFD_FACE_XM) && x < W) || ((pml_faces & AFD_FACE_XP) && x > nx - W - 1))
+                        ax |= 1u;
+                    if (((pml_faces & AFD_FACE_YM) && y < W) || ((pml_faces & AFD_FACE_YP) && y > ny - W - 1))
+                        ax |= 2u;
+                    if (((pml_faces & AFD_FACE_ZM) && z < W) || ((pml_faces & AFD_FACE_ZP) && z > nz - W - 1))
+                        ax |= 4u;
+                    if (!ax) continue;
+                    if (is_lrs[((size_t)z * ny + y) * nx + x]) continue;
+                    if (have_model && x < model.nx && y < model.ny && z < model.nz && model.at(x, y, z) != -1)
+                        continue;
+                    cells.push_back((int32_t)(z * plane + y * pitch + x));
+                    flags.push_back((uint8_t)ax);
+                }
+        pml_cells.upload(cells);
+        pml_flags.upload(flags);
+        n_pml_cells = (int64_t)cells.size();
+    }
+}
+
+void Engine::Impl::upload_sources() {
+    std::vector<int32_t> cell, begin((size_t)prm.batch + 1, 0);
+    std::vector<int64_t> off, len;
+    std::vector<float> data;
+    for (int32_t b = 0; b < prm.batch; ++b) {
+        begin[(size_t)b] = (int32_t)cell.size();
+        for (const Source& s : sources) {
+            if (s.batch != b) continue;
+            check_cell(s.ijk, nx, ny, nz, "source");
+            cell.push_back((int32_t)(s.ijk[2] * plane + s.ijk[1] * pitch + s.ijk[0]));
+            off.push_back((int64_t)data.size());
+            len.push_back((int64_t)s.sig.size());
+            data.insert(data.end(), s.sig.begin(), s.sig.end());
+        }
+    }
+    begin[(size_t)prm.batch] = (int32_t)cell.size();
+    src_cell.upload(cell);
+    src_begin.upload(begin);
+    src_off.upload(off);
+    src_len.upload(len);
+    if (data.empty()) data.push_back(0.0f);
+    src_data.upload(data);
+    src_dirty = false;
+}
+
+// CheckVariables (simulation.hpp:436-447): the receiver record grows to the
+// new end time; recorded samples keep their place.
+void Engine::Impl::ensure_receivers(int64_t t_end) {
+    const int32_t nr = (int32_t)receivers.size();
+    if (nr == rcv_n_dev && rcv_cap >= t_end && rcv_out.ptr) return;
+    std::vector<int32_t> cell;
+    for (auto& r : receivers) {
+        check_cell(r.data(), nx, ny, nz, "receiver");
+        cell.push_back((int32_t)(r[2] * plane + r[1] * pitch + r[0]));
+    }
+    int64_t cap = std::max<int64_t>(t_end, 1);
+    cap = std::max(cap, rcv_cap);
+    DBuf<float> fresh;
+    fresh.alloc((size_t)prm.batch * std::max(nr, 1) * cap);
+    if (rcv_out.ptr && rcv_cap > 0 && steps_done > 0) {
+        // copy the rows of the receivers that existed before
+        for (int32_t b = 0; b < prm.batch; ++b)
+            CK(cudaMemcpy2D(fresh.ptr + (size_t)b * nr * cap, cap * sizeof(float),
+                            rcv_out.ptr + (size_t)b * rcv_n_dev * rcv_cap, rcv_cap * sizeof(float),
+                            steps_done * sizeof(float), (size_t)rcv_n_dev, cudaMemcpyDeviceToDevice));
+    }
+    std::swap(rcv_out.ptr, fresh.ptr);
+    std::swap(rcv_out.n, fresh.n);
+    rcv_cap = cap;
+    rcv_n_dev = nr;
+    rcv_cell.upload(cell);
+    drop_graphs();
+}
+
+void Engine::Impl::build_args() {
+    StepArgs& a = args;
+    a = StepArgs{};
+    a.g = GridDev{nx, ny, nz, pitch, plane, vol};
+    a.batch = prm.batch;
+    a.mode = prm.mode;
+    for (int k = 0; k < 3; ++k) a.p[k] = fields.ptr + (size_t)k * vol * prm.batch;
+    a.d_step = d_step.ptr;
+    a.lambda2 = lambda2();
+    a.cint = 2.0f * (1.0f - 3.0f * a.lambda2);
+    a.lrs.n = (int32_t)lrs_cell.n;
+    a.lrs.K = have_model ? model.ncoef : 1;
+    a.lrs.S = 3 * a.lrs.K;
+    a.lrs.cell = lrs_cell.ptr;
+    a.lrs.info = lrs_info.ptr;
+    a.lrs.st_in = lrs_in.ptr;
+    a.lrs.st_out = lrs_out.ptr;
+    a.lrs.ca = coef_a.ptr;
+    a.lrs.cb = coef_b.ptr;
+    // REF: simulation.hpp:368-369 passes lambda^2 as l (lrs_1.cl:58,78)
+    a.lrs.l = ref() ? a.lambda2 : prm.dt * prm.c / prm.dx;
+    a.lrs.l2 = a.lrs.l * a.lrs.l;
+    a.lrs.c2 = 2.0f * (1.0f - 3.0f * a.lrs.l2);
+    PmlDev& P = a.pml;
+    P.width = pml_width > 0 && psi[0].ptr ? pml_width : 0;
+    P.faces = pml_faces;
+    P.g0 = pml_g0;
+    for (int x = 0; x < 3; ++x) {
+        P.fi[x][0] = fi[x][0].ptr;
+        P.fi[x][1] = fi[x][1].ptr;
+        P.ksi[x] = ksi_dev[x].ptr;
+    }
+    P.psi[0] = psi[0].ptr;
+    P.psi[1] = psi[1].ptr;
+    P.n_cells = (int32_t)n_pml_cells;
+    P.cells = pml_cells.ptr;
+    P.flags = pml_flags.ptr;
+    const float c = prm.c, dx = prm.dx, dt = prm.dt;
+    P.dt = dt;
+    P.cc_dxdx = c * c / (dx * dx);
+    P.inv_dx = 1.0f / dx;
+    P.half_inv_dx = 0.5f / dx;
+    P.inv_dt2 = 1.0f / (dt * dt);
+    P.two_dt = 2.0f * dt;
+    P.inv_dt = 1.0f / dt;
+    a.src.n = (int32_t)src_cell.n;
+    a.src.cell = src_cell.ptr;
+    a.src.begin = src_begin.ptr;
+    a.src.off = src_off.ptr;
+    a.src.len = src_len.ptr;
+    a.src.data = src_data.ptr;
+    a.rcv.n = rcv_n_dev;
+    a.rcv.cell = rcv_cell.ptr;
+    a.rcv.out = rcv_out.ptr;
+    a.rcv.cap = rcv_cap;
+    a.flag = d_flag.ptr;
+}
+
+enum KernelKind { KK_INTERIOR, KK_LRS, KK_PML_AUX, KK_PML_P, KK_SRC_RCV, KK_COUNT };
+static const char* kKernelNames[KK_COUNT] = {"interior", "boundary", "pml_aux", "pml_pressure",
+                                             "source_receiver"};
+
+// One time step, global step = *d_step + j (simulation.hpp:358-392).
+void Engine::Impl::launch_step(int j, bool profile) {
+    const StepArgs& a = args;
+    auto begin = [&](int kind) {
+        if (!profile) return;
+        if (ev_kind.size() >= ev_pool.size()) {
+            cudaEvent_t e0, e1;
+            CK(cudaEventCreate(&e0));
+            CK(cudaEventCreate(&e1));
+            ev_pool.emplace_back(e0, e1);
+        }
+        CK(cudaEventRecord(ev_pool[ev_kind.size()].first, stream));
+        ev_kind.push_back(kind);
+    };
+    auto end = [&]() {
+        if (!profile) return;
+        CK(cudaEventRecord(ev_pool[ev_kind.size() - 1].second, stream));
+    };
+    const dim3 blk(64, 4, 1);
+    {
+        const dim3 grd((unsigned)((nx - 2 + 63) / 64), (unsigned)((ny - 2 + 3) / 4),
+                       (unsigned)((nz - 2) * prm.batch));
+        begin(KK_INTERIOR);
+        k_interior<<<grd, blk, 0, stream>>>(a, j);
+        end();
+        ++launches;
+    }
+    if (a.lrs.n > 0) {
+        const dim3 grd((unsigned)((a.lrs.n + 255) / 256), (unsigned)prm.batch);
+        begin(KK_LRS);
+        if (ref()) k_lrs<true><<<grd, 256, 0, stream>>>(a, j);
+        else k_lrs<false><<<grd, 256, 0, stream>>>(a, j);
+        end();
+        ++launches;
+    }
+    if (a.pml.width > 0) {
+        if (ref()) {
+            if (nx > 4 && ny > 4 && nz > 4) {
+                const dim3 grd((unsigned)((nx - 4 + 63) / 64), (unsigned)((ny - 4 + 3) / 4),
+                               (unsigned)((nz - 4) * prm.batch));
+                begin(KK_PML_AUX);
+                k_pml_ref_aux<<<grd, blk, 0, stream>>>(a, j);
+                end();
+                begin(KK_PML_P);
+                k_pml_ref_p<<<grd, blk, 0, stream>>>(a, j);
+                end();
+                launches += 2;
+            }
+        } else if (a.pml.n_cells > 0) {
+            const dim3 grd((unsigned)((a.pml.n_cells + 255) / 256), (unsigned)prm.batch);
+            begin(KK_PML_P);
+            k_pml_fix_p<<<grd, 256, 0, stream>>>(a, j);
+            end();
+            begin(KK_PML_AUX);
+            k_pml_fix_aux<<<grd, 256, 0, stream>>>(a, j);
+            end();
+            launches += 2;
+        }
+    }
+    if (a.src.n > 0 || a.rcv.n > 0) {
+        begin(KK_SRC_RCV);
+        k_src_rcv<<<(unsigned)prm.batch, 128, 0, stream>>>(a, j);
+        end();
+        ++launches;
+    }
+}
+
+cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
+    auto it = graphs.find(n);
+    if (it != graphs.end()) return it->second;
+    cudaGraph_t graph;
+    const int64_t saved = launches;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int64_t j = 0; j < n; ++j) launch_step((int)j, false);
+    k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
+    CK(cudaStreamEndCapture(stream, &graph));
+    launches = saved;
+    cudaGraphExec_t exec;
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    graphs[n] = exec;
+    return exec;
+}
+
+void Engine::Impl::run_chunk(int64_t n) {
+    const bool profile = prm.profile != 0;
+    if (prm.graphs && !profile) {
+        cudaGraphExec_t g = graph_for(n);
+        CK(cudaGraphLaunch(g, stream));
+        // the graph holds n steps of kernels plus the step-counter advance
+        const int64_t before = launches;
+        launch_step_count_only(n);
+        (void)before;
+    } else {
+        for (int64_t j = 0; j < n; ++j) launch_step((int)j, profile);
+        k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
+        ++launches;
+    }
+    CK(cudaGetLastError());
+}
+
+void Engine::Impl::collect_profile() {
+    if (ev_kind.empty()) return;
+    CK(cudaStreamSynchronize(stream));
+    for (size_t k = 0; k < ev_kind.size(); ++k) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, ev_pool[k].first, ev_pool[k].second));
+        KernelStat& st = kstats[(size_t)ev_kind[k]];
+        st.launches += 1;
+        st.ms += ms;
+    }
+    ev_kind.clear();
+}
+
+int64_t Engine::Impl::kernels_per_step() const {
+    const StepArgs& a = args;
+    int64_t k = 1;
+    if (a.lrs.n > 0) ++k;
+    if (a.pml.width > 0) {
+        if (ref()) k += (nx > 4 && ny > 4 && nz > 4) ? 2 : 0;
+        else if (a.pml.n_cells > 0) k += 2;
+    }
+    if (a.src.n > 0 || a.rcv.n > 0) ++k;
+    return k;
+}
+
+// ---------------------------------------------------------------------------
+// Engine public methods
+// ---------------------------------------------------------------------------
+Engine::Engine(const afd_params& p) : d_(new Impl) {
+    Impl& D = *d_;
+    D.prm = p;
+    if (!(p.dx > 0.0f) || !(p.c > 0.0f) || !(p.dt > 0.0f))
+        throw Error(AFD_ERR_ARG, "dx, c and dt must be positive");
+    if (p.batch < 1 || p.batch > 4096) throw Error(AFD_ERR_ARG, "batch must be in 1..4096");
+    if (p.mode != AFD_MODE_REF && p.mode != AFD_MODE_FIXED) throw Error(AFD_ERR_ARG, "unknown mode");
+    if (p.storage != AFD_STORE_FP32) throw Error(AFD_ERR_ARG, "unsupported storage");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Error(AFD_ERR_CUDA, "no CUDA device available");
+    if (p.device < 0 || p.device >= ndev) throw Error(AFD_ERR_ARG, "device ordinal out of range");
+    D.device = p.device;
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamCreateWithFlags(&D.own_stream, cudaStreamNonBlocking));
+    D.stream = D.own_stream;
+    CK(cudaEventCreate(&D.ev0));
+    CK(cudaEventCreate(&D.ev1));
+    D.d_step.alloc(1);
+    D.d_flag.alloc(1);
+    D.d_energy.alloc(1);
+    CK(cudaMemcpyToSymbol(c_group_mask, kGroupMask, sizeof(kGroupMask)));
+    for (int k = 0; k < KK_COUNT; ++k) D.kstats.push_back(KernelStat{kKernelNames[k], 0, 0.0});
+}
+
+Engine::~Engine() {
+    Impl& D = *d_;
+    cudaSetDevice(D.device);
+    if (D.stream) cudaStreamSynchronize(D.stream);
+    D.drop_graphs();
+    for (auto& e : D.ev_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    if (D.ev0) cudaEventDestroy(D.ev0);
+    if (D.ev1) cudaEventDestroy(D.ev1);
+    if (D.own_stream) cudaStreamDestroy(D.own_stream);
+}
+
+float Engine::cell_size() const { return d_->prm.dx; }
+
+void Engine::set_stream(void* stream) {
+    Impl& D = *d_;
+    CK(cudaSetDevice(D.device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : D.own_stream;
+    if (s != D.stream) {
+        CK(cudaStreamSynchronize(D.stream));
+        D.drop_graphs();
+        D.stream = s;
+    }
+}
+
+void Engine::set_min_size(float x, float y, float z) {
+    Impl& D = *d_;
+    if (D.initialized) throw Error(AFD_ERR_STATE, "the grid is fixed after the first run");
+    const float v[3] = {x, y, z};
+    int32_t out[3];
+    for (int k = 0; k < 3; ++k) {
+        if (!(v[k] >= 0.0f) || !(v[k] / D.prm.dx < 65536.0f)) throw Error(AFD_ERR_ARG, "minsize out of range");
+        out[k] = (int32_t)round_to((uint32_t)(cell_of(v[k], D.prm.dx) + 1), 32);
+    }
+    std::copy(out, out + 3, D.min_size);
+}
+
+void Engine::set_model(const Model& m) {
+    Impl& D = *d_;
+    if (D.initialized) throw Error(AFD_ERR_STATE, "the model cannot change after the first run");
+    if (m.nx < 3 || m.ny < 3 || m.nz < 3) throw Error(AFD_ERR_ARG, "model grid must be at least 3x3x3");
+    if (m.nmat < 1 || m.nmat > 256) throw Error(AFD_ERR_ARG, "1..256 materials are supported");
+    if (m.ncoef < 1 || m.ncoef > 64) throw Error(AFD_ERR_ARG, "filters must have 1..64 coefficients");
+    for (int64_t k = 0; k < m.cells(); ++k)
+        if (m.vox[(size_t)k] < -1 || m.vox[(size_t)k] >= m.nmat)
+            throw Error(AFD_ERR_ARG, "voxel material index out of range");
+    std::vector<BoundaryPoint> pts = classify(m);
+    D.model = m;
+    D.boundary.swap(pts);
+    D.have_model = true;
+}
+
+void Engine::set_pml(int32_t width, uint32_t faces, const float* kx, const float* ky, const float* kz) {
+    Impl& D = *d_;
+    if (width < 0) throw Error(AFD_ERR_ARG, "PML width must be >= 0");
+    int32_t dims[3];
+    D.grid_dims(dims);
+    if (width > 0 && (dims[0] < 3 || dims[1] < 3 || dims[2] < 3))
+        throw Error(AFD_ERR_STATE, "load a model or set minsize before pml");
+    const float* src[3] = {kx, ky, kz};
+    for (int k = 0; k < 3; ++k) {
+        D.ksi[k].assign((size_t)std::max(dims[k], 0), 0.0f);
+        if (src[k] && dims[k] > 0) std::copy(src[k], src[k] + dims[k], D.ksi[k].begin());
+    }
+    D.pml_width = width;
+    D.pml_faces = faces & 63u;
+    D.pml_dirty = true;
+}
+
+void Engine::set_pml_profile(int32_t width, const float* prof, int32_t len) {
+    Impl& D = *d_;
+    if (len < 0 || (len > 0 && !prof)) throw Error(AFD_ERR_ARG, "bad PML profile");
+    int32_t dims[3];
+    D.grid_dims(dims);
+    if (dims[0] < 3 || dims[1] < 3 || dims[2] < 3)
+        throw Error(AFD_ERR_STATE, "load a model or set minsize before pml");
+    std::vector<float> k3[3];
+    for (int k = 0; k < 3; ++k) {
+        k3[k].assign((size_t)dims[k], 0.0f);
+        // simulation.hpp:268-276: ksi[i] = ksi[n-1-i] = prof[L-1-i]
+        for (int32_t i = 0; i < len; ++i) {
+            if (i >= dims[k]) throw Error(AFD_ERR_ARG, "PML profile longer than the grid");
+            k3[k][(size_t)i] = prof[len - 1 - i];
+            k3[k][(size_t)(dims[k] - i - 1)] = prof[len - 1 - i];
+        }
+    }
+    set_pml(width, 63u, k3[0].data(), k3[1].data(), k3[2].data());
+}
+
+void Engine::add_source_cell(int32_t batch, const int32_t ijk[3], const float* sig, int64_t len) {
+    Impl& D = *d_;
+    if (batch < 0 || batch >= D.prm.batch) throw Error(AFD_ERR_ARG, "batch index out of range");
+    if (len < 0 || (len > 0 && !sig)) throw Error(AFD_ERR_ARG, "bad source signal");
+    int32_t dims[3];
+    D.grid_dims(dims);
+    if (dims[0] > 0 && dims[1] > 0 && dims[2] > 0) check_cell(ijk, dims[0], dims[1], dims[2], "source");
+    Source s;
+    s.batch = batch;
+    std::copy(ijk, ijk + 3, s.ijk);
+    s.sig.assign(sig, sig + len);
+    D.sources.push_back(std::move(s));
+    D.src_dirty = true;
+}
+
+void Engine::add_source_pos(int32_t batch, const float pos[3], const float* sig, int64_t len) {
+    // (cl_int)(pos / res_), simulation.hpp:322
+    int32_t ijk[3];
+    for (int k = 0; k < 3; ++k) {
+        const float q = pos[k] / d_->prm.dx;
+        if (!(q > -2.0e9f && q < 2.0e9f)) throw Error(AFD_ERR_ARG, "source position out of range");
+        ijk[k] = (int32_t)q;
+    }
+    add_source_cell(batch, ijk, sig, len);
+}
+
+void Engine::add_receiver_cell(const int32_t ijk[3]) {
+    Impl& D = *d_;
+    int32_t dims[3];
+    D.grid_dims(dims);
+    if (dims[0] > 0 && dims[1] > 0 && dims[2] > 0) check_cell(ijk, dims[0], dims[1], dims[2], "receiver");
+    D.receivers.push_back({ijk[0], ijk[1], ijk[2]});
+}
+
+void Engine::add_receiver_pos(const float pos[3]) {
+    // (cl_int)(pos / res_), simulation.hpp:338
+    int32_t ijk[3];
+    for (int k = 0; k < 3; ++k) {
+        const float q = pos[k] / d_->prm.dx;
+        if (!(q > -2.0e9f && q < 2.0e9f)) throw Error(AFD_ERR_ARG, "receiver position out of range");
+        ijk[k] = (int32_t)q;
+    }
+    add_receiver_cell(ijk);
+}
+
+// Simulation::Run (simulation.hpp:342-434). Chunks end where the reference
+// reports progress (step 0 and every 200th step), so a chunk is one
+// captured graph replay; the REF-mode PML fields are zeroed after every
+// 8000th step of the run (simulation.hpp:411-430).
+int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
+    Impl& D = *d_;
+    if (steps < 0) throw Error(AFD_ERR_ARG, "steps must be >= 0");
+    CK(cudaSetDevice(D.device));
+    if (!D.initialized) D.init_device();
+    if (D.pml_dirty) {
+        D.setup_pml();
+        D.drop_graphs();
+    }
+    if (D.src_dirty) {
+        D.upload_sources();
+        D.drop_graphs();
+    }
+    D.ensure_receivers(D.steps_done + steps);
+    D.build_args();
+    D.launches = 0;
+    for (auto& st : D.kstats) {
+        st.launches = 0;
+        st.ms = 0.0;
+    }
+    CK(cudaMemsetAsync(D.d_flag.ptr, 0, sizeof(int), D.stream));
+    CK(cudaEventRecord(D.ev0, D.stream));
+    int status = AFD_OK;
+    int64_t i = 0;
+    while (i < steps) {
+        const int64_t n = (i == 0) ? 1 : std::min<int64_t>(200, steps - i);
+        D.run_chunk(n);
+        i += n;
+        const int64_t last = i - 1;
+        if (D.ref() && D.args.pml.width > 0 && last % 8000 == 0) {
+            const size_t bytes = (size_t)D.vol * D.prm.batch * sizeof(float);
+            for (int a = 0; a < 3; ++a)
+                for (int l = 0; l < 2; ++l) CK(cudaMemsetAsync(D.fi[a][l].ptr, 0, bytes, D.stream));
+            CK(cudaMemsetAsync(D.psi[0].ptr, 0, bytes, D.stream));
+            CK(cudaMemsetAsync(D.psi[1].ptr, 0, bytes, D.stream));
+        }
+        if (last % 200 == 0) {
+            if (D.prm.profile) D.collect_profile();
+            CK(cudaStreamSynchronize(D.stream));
+            int flag = 0;
+            CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+            if (flag && D.prm.watchdog) {
+                D.steps_done += i;
+                throw Error(AFD_ERR_NUMERIC, "pressure left the finite bound |p| < 1e30 by step " +
+                                                 std::to_string(D.steps_done));
+            }
+            if (cb && cb(last, steps, user) != 0) {
+                status = AFD_ERR_ABORTED;
+                break;
+            }
+        }
+    }
+    CK(cudaEventRecord(D.ev1, D.stream));
+    if (D.prm.profile) D.collect_profile();
+    CK(cudaEventSynchronize(D.ev1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, D.ev0, D.ev1));
+    D.last_ms = ms;
+    CK(cudaGetLastError());
+    int flag = 0;
+    CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    D.steps_done += i;
+    if (flag && D.prm.watchdog)
+        throw Error(AFD_ERR_NUMERIC,
+                    "pressure left the finite bound |p| < 1e30 by step " + std::to_string(D.steps_done));
+    if (status == AFD_OK && cb) cb(steps, steps, user);
+    return status;
+}
+
+void Engine::get_receivers(int32_t batch, float* out, int64_t cap) {
+    Impl& D = *d_;
+    if (batch < 0 || batch >= D.prm.batch) throw Error(AFD_ERR_ARG, "batch index out of range");
+    const int64_t nr = (int64_t)D.receivers.size();
+    const int64_t need = nr * D.steps_done;
+    if (cap < need) throw Error(AFD_ERR_ARG, "output buffer too small: need " + std::to_string(need));
+    if (need == 0) return;
+    if (D.rcv_n_dev != nr) throw Error(AFD_ERR_STATE, "receivers were added after the last run");
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamSynchronize(D.stream));
+    CK(cudaMemcpy2D(out, D.steps_done * sizeof(float),
+                    D.rcv_out.ptr + (size_t)batch * nr * D.rcv_cap, D.rcv_cap * sizeof(float),
+                    D.steps_done * sizeof(float), (size_t)nr, cudaMemcpyDeviceToHost));
+}
+
+void Engine::get_receivers_range(int32_t batch, int64_t t0, int64_t t1, float* out, int64_t cap) {
+    Impl& D = *d_;
+    if (batch < 0 || batch >= D.prm.batch) throw Error(AFD_ERR_ARG, "batch index out of range");
+    if (t0 < 0 || t1 < t0 || t1 > D.steps_done) throw Error(AFD_ERR_ARG, "time range outside the run");
+    const int64_t nr = (int64_t)D.receivers.size();
+    const int64_t n = t1 - t0;
+    if (cap < nr * n) throw Error(AFD_ERR_ARG, "output buffer too small");
+    if (nr == 0 || n == 0) return;
+    if (D.rcv_n_dev != nr) throw Error(AFD_ERR_STATE, "receivers were added after the last run");
+    CK(cudaSetDevice(D.device));
+    CK(cudaMemcpy2DAsync(out, n * sizeof(float), D.rcv_out.ptr + (size_t)batch * nr * D.rcv_cap + t0,
+                         D.rcv_cap * sizeof(float), n * sizeof(float), (size_t)nr, cudaMemcpyDeviceToHost,
+                         D.stream));
+    CK(cudaStreamSynchronize(D.stream));
+}
+
+// Replaces samples t0.. of one source. When the device copy already holds
+// the source at a sufficient length the new samples are copied in place
+// (stream-ordered with the steps already queued); otherwise the source
+// list is rebuilt at the next run.
+void Engine::update_source(int64_t index, int64_t t0, const float* sig, int64_t len) {
+    Impl& D = *d_;
+    if (index < 0 || index >= (int64_t)D.sources.size()) throw Error(AFD_ERR_ARG, "source index out of range");
+    if (t0 < 0) throw Error(AFD_ERR_ARG, "t0 must be >= 0");
+    Source& s = D.sources[(size_t)index];
+    const bool grows = (int64_t)s.sig.size() < t0 + len;
+    if (grows) s.sig.resize((size_t)(t0 + len), 0.0f);
+    std::copy(sig, sig + len, s.sig.begin() + t0);
+    if (grows || D.src_dirty || !D.src_data.ptr) {
+        D.src_dirty = true;
+        return;
+    }
+    // device position of this source: sources are stored grouped by batch member
+    int64_t off = 0;
+    for (int32_t b = 0; b < D.prm.batch; ++b)
+        for (const Source& q : D.sources) {
+            if (q.batch != b) continue;
+            if (&q == &s) {
+                CK(cudaSetDevice(D.device));
+                CK(cudaMemcpyAsync(D.src_data.ptr + off + t0, sig, (size_t)len * sizeof(float),
+                                   cudaMemcpyHostToDevice, D.stream));
+                return;
+            }
+            off += (int64_t)q.sig.size();
+        }
+}
+
+static const float* latest_field(Engine::Impl& D, int32_t batch) {
+    if (D.steps_done == 0) return nullptr;
+    const long long g = D.steps_done - 1;
+    return D.fields.ptr + (size_t)buf_new(g) * D.vol * D.prm.batch + (size_t)batch * D.vol;
+}
+
+void Engine::get_field(int32_t batch, float* out, int64_t cap) {
+    Impl& D = *d_;
+    if (!D.initialized) throw Error(AFD_ERR_STATE, "no field before the first run");
+    if (batch < 0 || batch >= D.prm.batch) throw Error(AFD_ERR_ARG, "batch index out of range");
+    const int64_t need = (int64_t)D.nx * D.ny * D.nz;
+    if (cap < need) throw Error(AFD_ERR_ARG, "output buffer too small");
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamSynchronize(D.stream));
+    const float* f = latest_field(D, batch);
+    if (!f) {
+        std::fill(out, out + need, 0.0f);
+        return;
+    }
+    CK(cudaMemcpy2D(out, D.nx * sizeof(float), f, D.pitch * sizeof(float), D.nx * sizeof(float),
+                    (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost));
+}
+
+void Engine::get_plane(int32_t batch, int32_t axis, int32_t index, float* out, int64_t cap) {
+    Impl& D = *d_;
+    if (!D.initialized) throw Error(AFD_ERR_STATE, "no field before the first run");
+    if (batch < 0 || batch >= D.prm.batch) throw Error(AFD_ERR_ARG, "batch index out of range");
+    const int32_t dims[3] = {D.nx, D.ny, D.nz};
+    if (axis < 0 || axis > 2 || index < 0 || index >= dims[axis]) throw Error(AFD_ERR_ARG, "bad plane");
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamSynchronize(D.stream));
+    const float* f = latest_field(D, batch);
+    int64_t rows, cols;
+    if (axis == 0) { rows = D.nz; cols = D.ny; }
+    else if (axis == 1) { rows = D.nz; cols = D.nx; }
+    else { rows = D.ny; cols = D.nx; }
+    if (cap < rows * cols) throw Error(AFD_ERR_ARG, "output buffer too small");
+    if (!f) {
+        std::fill(out, out + rows * cols, 0.0f);
+        return;
+    }
+    if (axis == 1) {
+        // copy_plane.cl:29-34: to[x, z] = from[x, level, z]
+        CK(cudaMemcpy2D(out, D.nx * sizeof(float), f + (size_t)index * D.pitch, D.plane * sizeof(float),
+                        D.nx * sizeof(float), (size_t)D.nz, cudaMemcpyDeviceToHost));
+    } else if (axis == 2) {
+        CK(cudaMemcpy2D(out, D.nx * sizeof(float), f + (size_t)index * D.plane, D.pitch * sizeof(float),
+                        D.nx * sizeof(float), (size_t)D.ny, cudaMemcpyDeviceToHost));
+    } else {
+        CK(cudaMemcpy2D(out, sizeof(float), f + index, D.pitch * sizeof(float), sizeof(float),
+                        (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost));
+    }
+}
+
+void Engine::get_info(afd_info* info) {
+    Impl& D = *d_;
+    std::memset(info, 0, sizeof(*info));
+    int32_t dims[3];
+    D.grid_dims(dims);
+    info->nx = dims[0];
+    info->ny = dims[1];
+    info->nz = dims[2];
+    info->ncoef = D.have_model ? D.model.ncoef : 0;
+    info->nmat = D.have_model ? D.model.nmat : 0;
+    info->batch = D.prm.batch;
+    info->steps_done = D.steps_done;
+    info->n_sources = (int64_t)D.sources.size();
+    info->n_receivers = (int64_t)D.receivers.size();
+    info->n_boundary = (int64_t)D.boundary.size();
+    int64_t counts[kNumGroups] = {};
+    for (const BoundaryPoint& b : D.boundary) counts[b.group]++;
+    for (int g = 0; g < kNumGroups; ++g) info->group_counts[g] = counts[g];
+    info->n_pml_cells = D.n_pml_cells;
+    info->lambda2 = D.lambda2();
+    info->mode = D.prm.mode;
+    info->storage = D.prm.storage;
+    info->last_run_ms = D.last_ms;
+    info->kernel_launches = D.launches;
+}
+
+int Engine::kernel_stats(int32_t idx, char* name, int64_t cap, int64_t* launches, double* ms) {
+    Impl& D = *d_;
+    if (idx < 0 || idx >= (int32_t)D.kstats.size()) return AFD_ERR_ARG;
+    const KernelStat& st = D.kstats[(size_t)idx];
+    if (name && cap > 0) {
+        std::strncpy(name, st.name.c_str(), (size_t)cap - 1);
+        name[cap - 1] = '\0';
+    }
+    if (launches) *launches = st.launches;
+    if (ms) *ms = st.ms;
+    return AFD_OK;
+}
+
+double Engine::energy(int32_t batch) {
+    Impl& D = *d_;
+    if (!D.initialized) throw Error(AFD_ERR_STATE, "no field before the first run");
+    if (batch < 0 || batch >= D.prm.batch) throw Error(AFD_ERR_ARG, "batch index out of range");
+    if (D.steps_done == 0) return 0.0;
+    CK(cudaSetDevice(D.device));
+    const long long g = D.steps_done - 1;
+    const size_t base = (size_t)batch * D.vol;
+    const size_t stride = (size_t)D.vol * D.prm.batch;
+    const float* u1 = D.fields.ptr + (size_t)buf_new(g) * stride + base;
+    const float* u0 = D.fields.ptr + (size_t)buf_cur(g) * stride + base;
+    CK(cudaMemsetAsync(D.d_energy.ptr, 0, sizeof(double), D.stream));
+    const dim3 blk(64, 4, 1);
+    const dim3 grd((unsigned)((D.nx - 2 + 63) / 64), (unsigned)((D.ny - 2 + 3) / 4), (unsigned)(D.nz - 2));
+    k_energy<<<grd, blk, 0, D.stream>>>(u1, u0, GridDev{D.nx, D.ny, D.nz, D.pitch, D.plane, D.vol},
+                                        (double)D.lambda2(), D.d_energy.ptr);
+    CK(cudaGetLastError());
+    double e = 0.0;
+    CK(cudaMemcpyAsync(&e, D.d_energy.ptr, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
+    CK(cudaStreamSynchronize(D.stream));
+    return e;
+}
+
+}  // namespace afd

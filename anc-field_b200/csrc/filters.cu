@@ -1,0 +1,166 @@
+// FP64 filter checks: polynomial roots by Durand-Kerner iteration and the
+// real part of the admittance on a dense frequency grid, one CUDA thread per
+// (material, frequency) and per material for the roots.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/afd.h"
+#include "filters.hpp"
+#include "model.hpp"
+
+namespace afd {
+
+namespace {
+
+struct C {
+    double re, im;
+};
+__host__ __device__ inline C cadd(C x, C y) { return {x.re + y.re, x.im + y.im}; }
+__host__ __device__ inline C csub(C x, C y) { return {x.re - y.re, x.im - y.im}; }
+__host__ __device__ inline C cmul(C x, C y) { return {x.re * y.re - x.im * y.im, x.re * y.im + x.im * y.re}; }
+__host__ __device__ inline C cdiv(C x, C y) {
+    const double d = y.re * y.re + y.im * y.im;
+    return {(x.re * y.re + x.im * y.im) / d, (x.im * y.re - x.re * y.im) / d};
+}
+__host__ __device__ inline double cabs_(C x) { return sqrt(x.re * x.re + x.im * x.im); }
+
+constexpr int kMaxCoef = 64;
+
+// Largest root magnitude of c[0] z^n + c[1] z^(n-1) + ... + c[n], n = K-1.
+__host__ __device__ double max_root_of(const double* c, int K) {
+    const int n = K - 1;
+    if (n <= 0) return 0.0;
+    if (c[0] == 0.0) return INFINITY;
+    C z[kMaxCoef];
+    double mono[kMaxCoef];
+    for (int k = 0; k <= n; ++k) mono[k] = c[k] / c[0];
+    C seed{0.4, 0.9}, p{1.0, 0.0};
+    for (int k = 0; k < n; ++k) {
+        z[k] = p;
+        p = cmul(p, seed);
+    }
+    for (int it = 0; it < 2000; ++it) {
+        double moved = 0.0;
+        for (int k = 0; k < n; ++k) {
+            C v{1.0, 0.0};  // Horner on the monic polynomial
+            for (int q = 1; q <= n; ++q) v = cadd(cmul(v, z[k]), C{mono[q], 0.0});
+            C den{1.0, 0.0};
+            for (int q = 0; q < n; ++q)
+                if (q != k) den = cmul(den, csub(z[k], z[q]));
+            const C step = cdiv(v, den);
+            z[k] = csub(z[k], step);
+            moved = fmax(moved, cabs_(step));
+        }
+        if (moved < 1e-15) break;
+    }
+    double m = 0.0;
+    for (int k = 0; k < n; ++k) m = fmax(m, cabs_(z[k]));
+    return m;
+}
+
+// Re{A(e^jw)/B(e^jw)}, coefficients in powers of z^-1.
+__host__ __device__ double re_admittance(const double* a, const double* b, int K, double w) {
+    C A{0.0, 0.0}, B{0.0, 0.0};
+    for (int k = 0; k < K; ++k) {
+        const C e{cos(-w * k), sin(-w * k)};
+        A = cadd(A, C{a[k] * e.re, a[k] * e.im});
+        B = cadd(B, C{b[k] * e.re, b[k] * e.im});
+    }
+    return cdiv(A, B).re;
+}
+
+__global__ void k_roots(const double* b, int nmat, int K, double* out) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < nmat) out[m] = max_root_of(b + (size_t)m * K, K);
+}
+
+__global__ void k_passive(const double* a, const double* b, int nmat, int K, int nf, double* out) {
+    const int m = blockIdx.y;
+    double lo = INFINITY;
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+        const double w = 3.141592653589793 * (double)f / (double)(nf - 1);
+        lo = fmin(lo, re_admittance(a + (size_t)m * K, b + (size_t)m * K, K, w));
+    }
+    for (int o = 16; o > 0; o >>= 1) lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    __shared__ double part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = lo;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = part[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) v = fmin(v, part[k]);
+        // atomic min on a double through its bit pattern is valid only for
+        // one sign, so each block writes its own slot
+        out[(size_t)m * gridDim.x + blockIdx.x] = v;
+    }
+}
+
+#define CKF(call)                                                                        \
+    do {                                                                                 \
+        cudaError_t e__ = (call);                                                        \
+        if (e__ != cudaSuccess) throw Error(AFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+    } while (0)
+
+}  // namespace
+
+void check_filters(int32_t nmat, int32_t K, const double* a, const double* b, int32_t nf, int32_t* status,
+                   double* min_real, double* max_root) {
+    if (K > kMaxCoef) throw Error(AFD_ERR_ARG, "at most 64 filter coefficients");
+    std::vector<double> roots((size_t)nmat), lows((size_t)nmat, INFINITY);
+    int ndev = 0;
+    const bool gpu = cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0;
+    if (gpu) {
+        const int blocks = 8;
+        double *da, *db, *dr, *dl;
+        const size_t nab = (size_t)nmat * K;
+        CKF(cudaMalloc(&da, nab * sizeof(double)));
+        CKF(cudaMalloc(&db, nab * sizeof(double)));
+        CKF(cudaMalloc(&dr, (size_t)nmat * sizeof(double)));
+        CKF(cudaMalloc(&dl, (size_t)nmat * blocks * sizeof(double)));
+        CKF(cudaMemcpy(da, a, nab * sizeof(double), cudaMemcpyHostToDevice));
+        CKF(cudaMemcpy(db, b, nab * sizeof(double), cudaMemcpyHostToDevice));
+        k_roots<<<(nmat + 63) / 64, 64>>>(db, nmat, K, dr);
+        k_passive<<<dim3(blocks, nmat), 256>>>(da, db, nmat, K, nf, dl);
+        CKF(cudaGetLastError());
+        std::vector<double> part((size_t)nmat * blocks);
+        CKF(cudaMemcpy(roots.data(), dr, (size_t)nmat * sizeof(double), cudaMemcpyDeviceToHost));
+        CKF(cudaMemcpy(part.data(), dl, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int m = 0; m < nmat; ++m)
+            for (int k = 0; k < blocks; ++k) lows[(size_t)m] = std::fmin(lows[(size_t)m], part[(size_t)m * blocks + k]);
+        cudaFree(da);
+        cudaFree(db);
+        cudaFree(dr);
+        cudaFree(dl);
+    } else {
+        for (int m = 0; m < nmat; ++m) {
+            roots[(size_t)m] = max_root_of(b + (size_t)m * K, K);
+            for (int f = 0; f < nf; ++f) {
+                const double w = 3.141592653589793 * (double)f / (double)(nf - 1);
+                lows[(size_t)m] = std::fmin(lows[(size_t)m], re_admittance(a + (size_t)m * K, b + (size_t)m * K, K, w));
+            }
+        }
+    }
+    for (int m = 0; m < nmat; ++m) {
+        int st = 0;
+        if (!(roots[(size_t)m] < 1.0)) st |= 1;
+        if (!(lows[(size_t)m] >= 0.0)) st |= 2;
+        status[m] = st;
+        if (min_real) min_real[m] = lows[(size_t)m];
+        if (max_root) max_root[m] = roots[(size_t)m];
+    }
+}
+
+int device_name(int32_t index, std::string* name) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AFD_ERR_CUDA;
+    if (index < 0 || index >= ndev) return AFD_ERR_ARG;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, index) != cudaSuccess) return AFD_ERR_CUDA;
+    *name = prop.name;
+    return AFD_OK;
+}
+
+}  // namespace afd

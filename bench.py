@@ -1,0 +1,277 @@
+"""Benchmark of the B200 FDTD step on the 512x384x320 single-source
+throughput workload (4 materials with third-order wall filters, 20 furniture
+boxes, PML on two faces, band-limited noise source, 32 receivers).
+
+One step = one time step of the whole grid. Prints one JSON line.
+  value : interior cell-updates/s (Mcell/s) over K device-timed steps,
+          inputs resident in HBM (three FP32 levels of 252 MB each, larger
+          than L2, so no flush is needed between steps)
+  e2e   : the same through the public API with the step's source samples
+          copied host->device and the receiver samples device->host
+  roofline: the step kernel's algorithmic bytes / its CUDA-event duration
+  cpu_baseline: the reference's own kernels (oracle/_ref) on host cores
+
+--impl reference times the reference's CPU kernels instead (rank 0 only).
+Multi-GPU: one independent replica per rank (the path has no exchange
+step), scaling "weak", value = all ranks' cell-updates / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference(cfg, steps, budget_s=25.0, precision="f32"):
+    """Times the reference's own kernels (oracle/_ref, REF semantics, no PML
+    kernel) on the workload's geometry with all host threads. The sample is
+    a z-slab of the grid sized to about budget_s seconds in total."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    impl = "ref" if oracle.available("ref", precision) else "ora"
+    nx, ny, nz = cfg.dims
+    # one probe step on a thin slab to size the sample
+    def run_slab(zs, n):
+        vox = cfg.vox[:zs].copy()
+        vox[-1] = np.where(vox[-1] == -1, 0, vox[-1])  # close the slab with a wall
+        import ancfield_b200.workloads as W
+        vox = W.close_gaps(vox)
+        src = [((cfg.sources[0][0][0], cfg.sources[0][0][1], min(cfg.sources[0][0][2], zs - 3)),
+                cfg.sources[0][1][:n])]
+        rcv = [(r[0], r[1], min(r[2], zs - 2)) for r in cfg.receivers]
+        t = time.perf_counter()
+        oracle.simulate((nx, ny, zs), vox, cfg.a, cfg.b, dx=cfg.dx, c=cfg.c, dt=cfg.dt, mode=0,
+                        sources=src, receivers=rcv, steps=n, impl=impl)
+        return time.perf_counter() - t
+    zs = min(nz, 16)
+    t1 = run_slab(zs, 2)
+    per_cell_step = t1 / (2 * nx * ny * zs)
+    zs = int(max(8, min(nz, budget_s / max(steps, 1) / (per_cell_step * nx * ny))))
+    t = run_slab(zs, steps)
+    cells = (nx - 2) * (ny - 2) * (zs - 2)
+    return {"value": cells * steps / t / 1e6, "unit": "Mcell-updates/s", "cores": os.cpu_count(),
+            "kind": "reference" if impl == "ref" else "port",
+            "sample": "%dx%dx%d slab of the workload grid, %d steps, reference kernels leapfrog+26 LRS+"
+                      "source+mic (REF semantics, PML kernel not run), OpenMP %d threads, %.1f s"
+                      % (nx, ny, zs, steps, os.cpu_count(), t)}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    import __graft_entry__ as ge
+    pkg = ge.load()
+    W = pkg.workloads
+    cfg = W.config_c2(steps=max(args.steps, 1))
+    nx, ny, nz = cfg.dims
+    interior = (nx - 2) * (ny - 2) * (nz - 2)
+    metric = "Mcell-updates/s"
+    config = {"workload": "512x384x320 single-source FP32 (4 materials K=4, 20 boxes, PML x+/z+ "
+                          "width 12, 32 receivers)", "grid": [nx, ny, nz], "interior_cells": interior,
+              "mode": "FIXED", "l2_flush": "not needed: three 252 MB field levels exceed the 126 MB L2",
+              "parallelism": "replicas" if world > 1 else "single"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_reference(cfg, max(args.steps, 1) + max(args.warmup, 0), budget_s=90.0)
+        line = {"metric": metric, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "impl": "reference", "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    stream = torch.cuda.Stream()
+
+    def make_sim(profile=0, graphs=1):
+        sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, device=local, profile=profile,
+                             graphs=graphs)
+        sim.SetModel(pkg.Model.from_voxels(cfg.vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
+        sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi)
+        sim.AddSourceCell(cfg.sources[0][0], cfg.sources[0][1])
+        for r in cfg.receivers:
+            sim.AddMicCell(r)
+        sim.set_stream(stream.cuda_stream)
+        return sim
+
+    sim = make_sim()
+    K, Wm = args.steps, max(args.warmup, 3)
+    sim.Run(Wm)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.Run(K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    launches = sim.info().kernel_launches
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = interior * K * world / (ms / 1e3) / 1e6
+
+    # end to end through the public API: per step the source sample goes
+    # host->device and the receiver samples come back device->host
+    chunk = 200
+    sig = np.ascontiguousarray(cfg.sources[0][1], dtype=np.float32)
+    host_rcv = np.empty((len(cfg.receivers), chunk), np.float32)
+    t_start = sim.info().steps_done
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    done = 0
+    while done < K:
+        n = min(chunk, K - done)
+        t0 = t_start + done
+        sim.update_source(0, t0, sig[(t0 % len(sig)):(t0 % len(sig)) + n]
+                          if (t0 % len(sig)) + n <= len(sig) else np.resize(sig, n))
+        sim.Run(n)
+        sim.mics_range(t0, t0 + n, out=host_rcv[:, :n] if n == chunk else None)
+        done += n
+    e2e_s = time.perf_counter() - w0
+    e2e_ms = e2e_s * 1e3
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": interior * K * world / (e2e_ms / 1e3) / 1e6, "unit": metric,
+           "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * len(cfg.receivers)}
+
+    # roofline of the dominant kernel: per-launch CUDA events (profile mode)
+    sim.close()
+    psim = make_sim(profile=1, graphs=0)
+    psim.Run(min(K, 400) + 1)
+    stats = psim.kernel_stats()
+    psim.close()
+    top = max(stats.items(), key=lambda kv: kv[1][1])
+    name, (n_launch, tot_ms) = top
+    avg_ms = tot_ms / max(n_launch, 1)
+    step_kernel_bytes = 12.0 * interior  # read p^n, read p^{n-1}, write p^{n+1}
+    peak, peak_kind = peaks()
+    achieved = step_kernel_bytes / (avg_ms / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(name)
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "bytes_per_launch": step_kernel_bytes, "avg_launch_ms": avg_ms,
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in stats.items()}}
+
+    line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": K, "warmup": Wm,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": config, "e2e": e2e, "roofline": roof,
+            "gpu_launches": launches, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference(cfg, 4)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

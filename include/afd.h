@@ -1,0 +1,251 @@
+/*
+ * afd.h - C ABI of the B200 acoustic FDTD core (anc-field drop-in).
+ *
+ * Two handle types:
+ *   afd_model  host-only geometry: Kerkythea XML -> int32 voxel grid plus
+ *              per-material admittance filter coefficients, and the
+ *              boundary (LRS) classification. Needs no GPU.
+ *   afd_sim    one simulation on one CUDA device: pressure fields, boundary
+ *              filter state, PML fields, sources, receivers, the step loop.
+ *
+ * Conventions
+ *   - Every call returns an int status: AFD_OK (0) or a negative AFD_ERR_*.
+ *     The message of the last failure is afd_last_error() /
+ *     afd_model_last_error(). No C++ exception crosses this boundary.
+ *   - The library copies every input; outputs go into caller buffers whose
+ *     capacity (in elements) is passed as `cap`.
+ *   - Grids are x-fastest: index(x,y,z) = (z*ny + y)*nx + x, as the
+ *     reference's clh macros define it (anc-field/clh/clh-kernel.hpp:238-248).
+ *   - One handle per host thread. Calls are synchronous.
+ *
+ * Reference interfaces replaced (paths inside szarvas/anc-field):
+ *   Simulation class   anc-field/src/simulation.hpp:83-156
+ *   Kerkythea loader   anc-field/src/kerkythea.hpp:133-196
+ *   LrsData            anc-field/src/lrs-data.hpp:116-215
+ *   clh::Kernel launch anc-field/clh/clh-kernel.hpp:163-183
+ */
+#ifndef AFD_H
+#define AFD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AFD_OK              0
+#define AFD_ERR_ARG        -1  /* bad argument, size or index */
+#define AFD_ERR_STATE      -2  /* call not valid in the current state */
+#define AFD_ERR_IO         -3  /* file missing or unparsable */
+#define AFD_ERR_GEOMETRY   -4  /* unphysical surfaces (lrs-data.hpp:327) */
+#define AFD_ERR_CUDA       -5  /* CUDA runtime failure or no device */
+#define AFD_ERR_NUMERIC    -6  /* watchdog: a pressure value left the finite bound */
+#define AFD_ERR_FILTER     -7  /* filter stability / passivity check failed */
+#define AFD_ERR_ABORTED    -8  /* the progress callback asked to stop */
+
+/* Boundary update semantics. */
+#define AFD_MODE_REF    0  /* the reference kernels' arithmetic, quirks included */
+#define AFD_MODE_FIXED  1  /* the intended scheme: quirks of the reference removed */
+
+/* Field storage precision. */
+#define AFD_STORE_FP32  0
+#define AFD_STORE_FP16  1
+
+/* PML face bits (FIXED mode; REF mode always uses all six ends). */
+#define AFD_FACE_XM 1u
+#define AFD_FACE_XP 2u
+#define AFD_FACE_YM 4u
+#define AFD_FACE_YP 8u
+#define AFD_FACE_ZM 16u
+#define AFD_FACE_ZP 32u
+
+/* The 26 boundary groups, numbered as lrs-data.hpp:53-78 numbers them. */
+#define AFD_NUM_GROUPS 26
+
+typedef struct afd_params {
+    float dx;          /* cell size in metres; also the position->cell divisor (ref 0.02) */
+    float c;           /* speed of sound, m/s (ref 340) */
+    float dt;          /* time step, s (ref 3.125e-5) */
+    float fs;          /* samples per second used by run-in-seconds callers (ref 32000) */
+    int32_t mode;      /* AFD_MODE_REF or AFD_MODE_FIXED */
+    int32_t storage;   /* AFD_STORE_FP32 or AFD_STORE_FP16 */
+    int32_t batch;     /* independent source sets sharing one geometry (>= 1) */
+    int32_t device;    /* CUDA device ordinal */
+    int32_t watchdog;  /* nonzero: stop a run whose field leaves |p| < 1e30 */
+    int32_t graphs;    /* nonzero: replay captured CUDA graphs of step chunks */
+    int32_t fused;     /* nonzero: one fused kernel per step; zero: one launch per sub-step */
+    int32_t profile;   /* nonzero: time every kernel launch with CUDA events (no graphs) */
+    int32_t reserved[4];
+} afd_params;
+
+/* Fills the reference constants: dx=0.02, c=340, dt=3.125e-5, fs=32000,
+ * REF mode, FP32, batch 1, device 0, watchdog on, graphs on, fused on. */
+void afd_default_params(afd_params* p);
+
+/* Version string of the library build. */
+const char* afd_version(void);
+
+/* Name of CUDA device `index` (the `lsd` listing, main.cpp:38-50).
+ * Returns AFD_ERR_ARG past the last device, AFD_ERR_CUDA without one. */
+int afd_device_name(int32_t index, char* out, int64_t cap);
+
+/* ------------------------------------------------------------------ */
+/* Host-only geometry                                                  */
+/* ------------------------------------------------------------------ */
+typedef struct afd_model afd_model;
+
+/* Kerkythea XML -> voxels + filters (replaces kerkythea.hpp:133-196 and
+ * LoadBoxes kerkythea.hpp:63-130). Material files <dir>/<name>_a.dat and
+ * _b.dat are read next to the XML, one coefficient per line. */
+int afd_model_load_kerkythea(afd_model** out, const char* xml_path, float res);
+
+/* Builds a model from a caller voxel grid (-1 air, else material index)
+ * and per-material coefficients a[nmat][ncoef], b[nmat][ncoef]. */
+int afd_model_from_voxels(afd_model** out, int32_t nx, int32_t ny, int32_t nz,
+                          const int32_t* vox, int32_t nmat, int32_t ncoef,
+                          const float* a, const float* b);
+
+/* dims[3] = {nx, ny, nz}; nmat, ncoef may be NULL. */
+int afd_model_dims(const afd_model* m, int32_t dims[3], int32_t* nmat, int32_t* ncoef);
+int afd_model_voxels(const afd_model* m, int32_t* out, int64_t cap);
+/* a and b each receive nmat*ncoef floats, material order = sorted names. */
+int afd_model_coefs(const afd_model* m, float* a, float* b, int64_t cap);
+/* Material names joined by '\n' (sorted as std::set sorts them). */
+int afd_model_material_names(const afd_model* m, char* out, int64_t cap);
+
+/* Boundary classification of lrs-data.hpp:116-215: counts[g] = number of
+ * air cells in group g. Fails with AFD_ERR_GEOMETRY on an unphysical
+ * pattern (opposite solid neighbours or more than three). */
+int afd_model_classify(const afd_model* m, int64_t counts[AFD_NUM_GROUPS]);
+/* Per-group point list {x,y,z,mat0,mat1,mat2} (unused mats = -1), in the
+ * reference's z-y-x scan order. n_out receives the point count. */
+int afd_model_group_points(const afd_model* m, int32_t group, int32_t* out,
+                           int64_t cap, int64_t* n_out);
+
+const char* afd_model_last_error(const afd_model* m);
+void afd_model_destroy(afd_model* m);
+
+/* FP64 admittance-filter check (run on the GPU when one is present, else
+ * on the host): stability = every root of b(z) (the recursion's
+ * denominator, coefficient order b0 + b1 z^-1 + ...) inside |z| < 1 - margin;
+ * passivity = Re{A(e^jw)/B(e^jw)} >= 0 on n_freq uniformly spaced
+ * frequencies in [0, pi]. status[i] bit0 = unstable, bit1 = not passive.
+ * min_real[i] receives the minimum real part found. */
+int afd_check_filters(int32_t nmat, int32_t ncoef, const double* a, const double* b,
+                      int32_t n_freq, int32_t* status, double* min_real, double* max_root);
+
+/* ------------------------------------------------------------------ */
+/* Simulation                                                          */
+/* ------------------------------------------------------------------ */
+typedef struct afd_sim afd_sim;
+
+/* Progress callback, called on the calling thread after step i (0-based,
+ * run-local) when i == 0 and every 200 steps, and once more with
+ * i == steps at the end (simulation.hpp:403-409, 433). A nonzero return
+ * stops the run with AFD_ERR_ABORTED after the current chunk. */
+typedef int (*afd_progress_fn)(int64_t i, int64_t steps, void* user);
+
+/* Replaces Simulation::Simulation (simulation.hpp:158-171). */
+int afd_create(afd_sim** out, const afd_params* p);
+
+/* Replaces Simulation::SetMinSize (simulation.hpp:279-284): each edge
+ * becomes RoundTo((int)(len/dx)+1, 32); the grid is the per-axis maximum
+ * of this and the model grid. */
+int afd_set_min_size(afd_sim* s, float x_m, float y_m, float z_m);
+
+/* Replaces Simulation::Load (simulation.hpp:173-199). */
+int afd_load(afd_sim* s, const char* xml_path);
+/* Same, from a model built by afd_model_* (the model is copied). */
+int afd_set_model(afd_sim* s, const afd_model* m);
+
+/* Replaces Simulation::SetPml (simulation.hpp:233-277). ksi_x/y/z hold nx,
+ * ny, nz damping values (1/s). REF mode: the whole interior 2..N-3 is
+ * updated by the PML kernel and the auxiliary fields in the end slabs of
+ * `width` cells (pml.cl:182, 231-262); face_mask is ignored. FIXED mode:
+ * only non-boundary air cells inside the slabs of the faces in face_mask.
+ * width 0 disables the PML. */
+int afd_set_pml(afd_sim* s, int32_t width, uint32_t face_mask,
+                const float* ksi_x, const float* ksi_y, const float* ksi_z);
+/* Builds the reference ksi arrays from a profile file's values as
+ * SetPml does (ksi[i] = ksi[n-1-i] = prof[L-1-i], i < L) and sets them. */
+int afd_set_pml_profile(afd_sim* s, int32_t width, const float* prof, int32_t len);
+
+/* Replaces Simulation::AddSource (simulation.hpp:309-324): the cell is
+ * (int)(pos/dx) per axis. Samples past len are zero. batch selects the
+ * source set (0 .. params.batch-1). */
+int afd_add_source(afd_sim* s, int32_t batch, const float pos_m[3],
+                   const float* signal, int64_t len);
+int afd_add_source_cell(afd_sim* s, int32_t batch, const int32_t ijk[3],
+                        const float* signal, int64_t len);
+
+/* Replaces Simulation::AddMic (simulation.hpp:326-340). Receivers are
+ * shared by every batch member. */
+int afd_add_receiver(afd_sim* s, const float pos_m[3]);
+int afd_add_receiver_cell(afd_sim* s, const int32_t ijk[3]);
+
+/* Replaces Simulation::Run (simulation.hpp:342-434): advances `steps`
+ * time steps; the time index continues across runs. */
+int afd_run(afd_sim* s, int64_t steps, afd_progress_fn cb, void* user);
+
+/* Receiver signals of one batch member, [n_receivers][t_end] row-major,
+ * t_end = total steps run so far (the `save` layout, datafile.hpp:87-94). */
+int afd_get_receivers(afd_sim* s, int32_t batch, float* out, int64_t cap);
+
+/* Streaming variants for callers that feed and drain a long run in parts:
+ * replaces the samples of source `index` (insertion order over all batch
+ * members) from time index t0 on (the signal grows when needed), and copies
+ * receiver samples t0 .. t1-1 of one batch member into out[n_receivers][t1-t0].
+ * Replace the clh host/device sync of simulation.hpp:95 and source.cl's
+ * argument upload for long runs split into parts. */
+int afd_update_source(afd_sim* s, int64_t index, int64_t t0, const float* signal, int64_t len);
+int afd_get_receivers_range(afd_sim* s, int32_t batch, int64_t t0, int64_t t1, float* out, int64_t cap);
+
+/* The latest pressure field p^n of one batch member, dense [nz][ny][nx]. */
+int afd_get_field(afd_sim* s, int32_t batch, float* out, int64_t cap);
+/* Headless 'vis': one plane of p^n (copy_plane.cl:29-34 takes axis 1).
+ * axis 0: out[nz][ny] at x=index; axis 1: out[nz][nx] at y=index;
+ * axis 2: out[ny][nx] at z=index. */
+int afd_get_plane(afd_sim* s, int32_t batch, int32_t axis, int32_t index,
+                  float* out, int64_t cap);
+
+typedef struct afd_info {
+    int32_t nx, ny, nz;          /* simulation grid */
+    int32_t ncoef, nmat;
+    int32_t batch;
+    int64_t steps_done;          /* global time index */
+    int64_t n_sources, n_receivers;
+    int64_t n_boundary;          /* LRS points, all groups */
+    int64_t group_counts[AFD_NUM_GROUPS];
+    int64_t n_pml_cells;         /* FIXED: cells with the PML update */
+    float lambda2;               /* (dt*c/dx)^2 in FP32 */
+    int32_t mode, storage;
+    double last_run_ms;          /* device time of the last afd_run (CUDA events) */
+    int64_t kernel_launches;     /* kernels launched by the last afd_run */
+    int32_t tile_x, tile_y, tile_z;  /* tile of the fused step kernel */
+    int32_t reserved[9];
+} afd_info;
+int afd_get_info(afd_sim* s, afd_info* info);
+
+/* Discrete energy of the SLF scheme, accumulated in FP64 on the GPU:
+ * kinetic + potential terms between the two latest time levels. */
+int afd_energy(afd_sim* s, int32_t batch, double* energy);
+
+/* Runs the simulation's work on the caller's CUDA stream (a cudaStream_t
+ * passed as void*), e.g. so that the caller can bracket afd_run with its own
+ * CUDA events. NULL restores the library's own stream. */
+int afd_set_stream(afd_sim* s, void* stream);
+
+/* Per-kernel statistics of the last afd_run made with params.profile set:
+ * kernel idx (0-based) -> name, launches and summed device milliseconds.
+ * Returns AFD_ERR_ARG when idx is past the last kernel. */
+int afd_kernel_stats(afd_sim* s, int32_t idx, char* name, int64_t cap,
+                     int64_t* launches, double* ms);
+
+const char* afd_last_error(const afd_sim* s);
+void afd_destroy(afd_sim* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AFD_H */
