@@ -48,6 +48,7 @@ struct PmlDev {
     // scalars, each computed on the host in FP32 exactly as the reference
     // kernel expression would compute it (pml.cl:185-262)
     float dt, cc_dxdx, inv_dx, half_inv_dx, inv_dt2, two_dt, inv_dt;
+    int32_t psi_on;    // psi is kept (REF always; FIXED with faces on all three axes)
 };
 
 struct SrcDev {
@@ -145,13 +146,15 @@ __constant__ uint8_t c_group_mask[26];
 // host call of simulation.hpp:368-369. FIXED: l is the Courant number,
 // corners use all three filters with a ring of K slots each, group 25 is a
 // regular corner.
-template <bool REF>
+// KT > 0 fixes the filter length at compile time (the tap loop unrolls and
+// all state loads issue together); KT = 0 reads it from L.K.
+template <bool REF, int KT = 0>
 __device__ __forceinline__ float lrs_point(const LrsDev& L, int e, int b, uint32_t info,
                                            const float nb[6], float pc, float pold, float pint,
                                            int ix_buf) {
     const int group = (int)(info & 31u);
     const int nf = group < 6 ? 1 : (group < 18 ? 2 : 3);
-    const int K = L.K;
+    const int K = KT > 0 ? KT : L.K;
     int mat[3] = {(int)((info >> 5) & 255u), (int)((info >> 13) & 255u), (int)((info >> 21) & 255u)};
     // ring width per filter: K, except REF corners (lrs_3.cl:70, size_a_0/2)
     const int size_f = (REF && nf == 3) ? K / 2 : K;
@@ -170,7 +173,7 @@ __device__ __forceinline__ float lrs_point(const LrsDev& L, int e, int b, uint32
             b0[f] = __ldg(L.cb + mat[f] * K);
         }
     }
-    for (int i = 1; i < K; ++i) {
+    auto tap = [&](int i) {
 #pragma unroll
         for (int f = 0; f < 3; ++f) {
             if (f < nf) {
@@ -180,6 +183,12 @@ __device__ __forceinline__ float lrs_point(const LrsDev& L, int e, int b, uint32
                 gn[f] += bi * sin_[(size_t)slot * n] - ai * sout[(size_t)slot * n];
             }
         }
+    };
+    if constexpr (KT > 0) {
+#pragma unroll
+        for (int i = 1; i < KT; ++i) tap(i);
+    } else {
+        for (int i = 1; i < K; ++i) tap(i);
     }
 
     const float l = L.l, l2 = L.l2;

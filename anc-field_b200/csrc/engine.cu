@@ -21,6 +21,7 @@
 
 #include "device.cuh"
 #include "engine.hpp"
+#include "fused.cuh"
 
 namespace afd {
 
@@ -86,8 +87,9 @@ __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
 
 // The 26 lrs_k launches of simulation.hpp:366-370 as one launch over the
 // compact list.
-template <bool REF>
-__global__ void __launch_bounds__(256) k_lrs(StepArgs a, int j) {
+// KT: filter length fixed at compile time (1..4), 0 for any length.
+template <bool REF, int KT>
+__global__ void __launch_bounds__(256) k_lrs(const __grid_constant__ StepArgs a, int j) {
     const long long g = *a.d_step + j;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.lrs.n) return;
@@ -96,13 +98,25 @@ __global__ void __launch_bounds__(256) k_lrs(StepArgs a, int j) {
     float* pn = a.p[buf_new(g)] + base;
     const float* pc = a.p[buf_cur(g)] + base;
     const float* po = a.p[buf_old(g)] + base;
-    const int64_t c = a.lrs.cell[e];
-    const uint32_t info = a.lrs.info[e];
-    const float nb[6] = {pc[c + 1], pc[c - 1], pc[c + a.g.pitch], pc[c - a.g.pitch],
-                         pc[c + a.g.plane], pc[c - a.g.plane]};
-    const float v = lrs_point<REF>(a.lrs, e, b, info, nb, pc[c], po[c], pn[c],
-                                   ring_index(g, a.lrs.K));
+    const int64_t c = __ldg(a.lrs.cell + e);
+    const uint32_t info = __ldg(a.lrs.info + e);
+    const float nb[6] = {__ldg(pc + c + 1), __ldg(pc + c - 1), __ldg(pc + c + a.g.pitch),
+                         __ldg(pc + c - a.g.pitch), __ldg(pc + c + a.g.plane), __ldg(pc + c - a.g.plane)};
+    const float pint = (REF && (info & 31u) == 25u) ? pn[c] : 0.0f;
+    const float v = lrs_point<REF, KT>(a.lrs, e, b, info, nb, __ldg(pc + c), __ldg(po + c), pint,
+                                       ring_index(g, a.lrs.K));
     pn[c] = v;
+}
+
+template <bool REF>
+static void launch_lrs(const StepArgs& a, int j, dim3 grd, cudaStream_t st) {
+    switch (a.lrs.K) {
+        case 1: k_lrs<REF, 1><<<grd, 256, 0, st>>>(a, j); break;
+        case 2: k_lrs<REF, 2><<<grd, 256, 0, st>>>(a, j); break;
+        case 3: k_lrs<REF, 3><<<grd, 256, 0, st>>>(a, j); break;
+        case 4: k_lrs<REF, 4><<<grd, 256, 0, st>>>(a, j); break;
+        default: k_lrs<REF, 0><<<grd, 256, 0, st>>>(a, j); break;
+    }
 }
 
 // ---- PML -------------------------------------------------------------------
@@ -179,10 +193,11 @@ __device__ __forceinline__ void pml_aux(const StepArgs& a, unsigned axes, const 
     const float kax = 0.5f * (P.ksi[0][x] + P.ksi[0][x + 1]);
     const float kay = 0.5f * (P.ksi[1][y] + P.ksi[1][y + 1]);
     const float kaz = 0.5f * (P.ksi[2][z] + P.ksi[2][z + 1]);
+    const bool psi = REF || P.psi_on;
     if (axes & 1u) {
         const float dxp = P.half_inv_dx * (Pn.ax(i + 1, pitch, plane) - Pn.ax(i, pitch, plane) +
                                            Pm.ax(i + 1, pitch, plane) - Plast.ax(i, pitch, plane));
-        const float dxpsi = P.inv_dx * (Ps.ax(i + 1, pitch, plane) - Ps.ax(i, pitch, plane));
+        const float dxpsi = psi ? P.inv_dx * (Ps.ax(i + 1, pitch, plane) - Ps.ax(i, pitch, plane)) : 0.0f;
         const float f1 = fx1[i];
         fx[i] = (-0.5f * kax * f1 + (kay + kaz - kax) * dxp + (kay * kaz) * dxpsi + P.inv_dt * f1) /
                 (P.inv_dt + kax * 0.5f);
@@ -190,7 +205,7 @@ __device__ __forceinline__ void pml_aux(const StepArgs& a, unsigned axes, const 
     if (axes & 2u) {
         const float dyp = P.half_inv_dx * (Pn.ay(i + pitch, pitch, plane) - Pn.ay(i, pitch, plane) +
                                            Pm.ay(i + pitch, pitch, plane) - Plast.ay(i, pitch, plane));
-        const float dypsi = P.inv_dx * (Ps.ay(i + pitch, pitch, plane) - Ps.ay(i, pitch, plane));
+        const float dypsi = psi ? P.inv_dx * (Ps.ay(i + pitch, pitch, plane) - Ps.ay(i, pitch, plane)) : 0.0f;
         const float kx_coef = REF ? 0.5f * (P.ksi[0][y] + P.ksi[0][y + 1]) : kax;
         const float f1 = fy1[i];
         fy[i] = (-0.5f * kay * f1 + (kax + kaz - kay) * dyp + (kx_coef * kaz) * dypsi + P.inv_dt * f1) /
@@ -199,7 +214,7 @@ __device__ __forceinline__ void pml_aux(const StepArgs& a, unsigned axes, const 
     if (axes & 4u) {
         const float dzp = P.half_inv_dx * (Pn.az(i + plane, pitch, plane) - Pn.az(i, pitch, plane) +
                                            Pm.az(i + plane, pitch, plane) - Plast.az(i, pitch, plane));
-        const float dzpsi = P.inv_dx * (Ps.az(i + plane, pitch, plane) - Ps.az(i, pitch, plane));
+        const float dzpsi = psi ? P.inv_dx * (Ps.az(i + plane, pitch, plane) - Ps.az(i, pitch, plane)) : 0.0f;
         const float f1 = fz1[i];
         fz[i] = (-0.5f * kaz * f1 + (kax + kay - kaz) * dzp + (kax * kay) * dzpsi + P.inv_dt * f1) /
                 (P.inv_dt + kaz * 0.5f);
@@ -266,36 +281,84 @@ __global__ void __launch_bounds__(256) k_pml_ref_p(StepArgs a, int j) {
     pn[i] = v;
 }
 
-// FIXED pass 1 (unfused order): pressure and psi of the PML cells.
-__global__ void __launch_bounds__(256) k_pml_fix_p(StepArgs a, int j) {
+// FIXED pass 1: pressure of the PML cells (pml.cl:185-207 on the PML
+// cells only). An auxiliary field is read only when its slab flags occur in
+// the cell's 2x2x2 cube x..x+1, y..y+1, z..z+1 (bits 3-5 of the flags);
+// elsewhere it is identically zero. psi is kept only when psi_on.
+__global__ void __launch_bounds__(256) k_pml_fix_p(const __grid_constant__ StepArgs a, int j) {
     const long long g = *a.d_step + j;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.pml.n_cells) return;
     const int b = blockIdx.y;
     const size_t base = (size_t)b * a.g.vol;
+    const PmlDev& P = a.pml;
+    const int64_t pitch = a.g.pitch, plane = a.g.plane;
     float* pn = a.p[buf_new(g)] + base;
     const float* pc = a.p[buf_cur(g)] + base;
     const float* po = a.p[buf_old(g)] + base;
     const int lv = pml_level(a, g);
-    const int64_t i = a.pml.cells[e];
-    const int z = (int)(i / a.g.plane);
-    const int y = (int)((i % a.g.plane) / a.g.pitch);
-    const int x = (int)(i % a.g.pitch);
-    float psi_new;
-    const float v = pml_pressure(a, pc, po, a.pml.fi[0][lv ^ 1] + base, a.pml.fi[1][lv ^ 1] + base,
-                                 a.pml.fi[2][lv ^ 1] + base, a.pml.psi[lv ^ 1] + base, x, y, z, i,
-                                 &psi_new);
-    a.pml.psi[lv][base + i] = psi_new;
+    const int64_t i = __ldg(P.cells + e);
+    const unsigned axes = __ldg(P.flags + e) >> 3;
+    const int z = (int)(i / plane);
+    const int y = (int)((i % plane) / pitch);
+    const int x = (int)(i % pitch);
+    const float kx = __ldg(P.ksi[0] + x), ky = __ldg(P.ksi[1] + y), kz = __ldg(P.ksi[2] + z);
+    const float pm1 = __ldg(pc + i), pm2 = __ldg(po + i);
+    float ps = 0.0f, pmh = 0.0f;
+    if (P.psi_on) {
+        pmh = P.psi[lv ^ 1][base + i];
+        ps = P.dt * pm1 + pmh;
+        P.psi[lv][base + i] = ps;
+    }
+    float s = __ldg(pc + i + 1) + __ldg(pc + i - 1);
+    s = s + __ldg(pc + i + pitch);
+    s = s + __ldg(pc + i - pitch);
+    s = s + __ldg(pc + i + plane);
+    s = s + __ldg(pc + i - plane);
+    s = s - 6.0f * pm1;
+    const float A = P.cc_dxdx * s;
+    float d = 0.0f;
+    if (axes & 1u) {
+        const float* f = P.fi[0][lv ^ 1] + base;
+        const float a1 = 0.25f * (((__ldg(f + i + 1) + __ldg(f + i + 1 + plane)) + __ldg(f + i + 1 + pitch)) +
+                                  __ldg(f + i + 1 + pitch + plane));
+        const float a0 = 0.25f * (((__ldg(f + i) + __ldg(f + i + plane)) + __ldg(f + i + pitch)) +
+                                  __ldg(f + i + pitch + plane));
+        d = a1 - a0;
+    }
+    if (axes & 2u) {
+        const float* f = P.fi[1][lv ^ 1] + base;
+        const int64_t q = i + pitch;
+        const float a1 = 0.25f * (((__ldg(f + q) + __ldg(f + q + plane)) + __ldg(f + q + 1)) + __ldg(f + q + 1 + plane));
+        const float a0 = 0.25f * (((__ldg(f + i) + __ldg(f + i + plane)) + __ldg(f + i + 1)) + __ldg(f + i + 1 + plane));
+        d = d + a1;
+        d = d - a0;
+    }
+    if (axes & 4u) {
+        const float* f = P.fi[2][lv ^ 1] + base;
+        const int64_t q = i + plane;
+        const float a1 = 0.25f * (((__ldg(f + q) + __ldg(f + q + pitch)) + __ldg(f + q + 1)) + __ldg(f + q + 1 + pitch));
+        const float a0 = 0.25f * (((__ldg(f + i) + __ldg(f + i + pitch)) + __ldg(f + i + 1)) + __ldg(f + i + 1 + pitch));
+        d = d + a1;
+        d = d - a0;
+    }
+    const float B = P.inv_dx * d;
+    const float C = kx * ky * kz * 0.5f * (ps + pmh);
+    const float D = P.inv_dt2 * (pm2 - 2.0f * pm1);
+    const float E = (kx * ky + ky * kz + kz * kx) * pm1;
+    const float F = (kx + ky + kz) / P.two_dt * pm2;
+    const float num = A + B - C - D - E + F;
+    const float v = num / (P.inv_dt2 + (kx + ky + kz) / P.two_dt);
     pn[i] = v;
     watch(a.flag, v);
 }
 
 // FIXED pass 2: auxiliary fields from the complete new pressure and psi.
-__global__ void __launch_bounds__(256) k_pml_fix_aux(StepArgs a, int j) {
+__global__ void __launch_bounds__(256) k_pml_fix_aux(const __grid_constant__ StepArgs a, int j) {
     const long long g = *a.d_step + j;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.pml.n_cells) return;
-    const unsigned axes = a.pml.flags[e];
+    const unsigned axes = __ldg(a.pml.flags + e) & 7u;
     if (!axes) return;
     const int b = blockIdx.y;
     const size_t base = (size_t)b * a.g.vol;
@@ -311,19 +374,166 @@ __global__ void __launch_bounds__(256) k_pml_fix_aux(StepArgs a, int j) {
                    a.pml.fi[1][lv] + base, a.pml.fi[2][lv] + base, x, y, z, i);
 }
 
+// ---------------------------------------------------------------------------
+// Fused step kernel (see fused.cuh for the structure)
+// ---------------------------------------------------------------------------
+// Interior SLF update of every cell 1..n-2 (leapfrog.cl:34-55) streamed
+// through shared memory; see fused.cuh. Consumer warps wait on the stage
+// barriers independently (no block-wide barrier), so a slow warp delays
+// only its own rows.
+__global__ void __launch_bounds__(F_THREADS, 2)
+    k_stream(const __grid_constant__ CUtensorMap tm_halo, const __grid_constant__ CUtensorMap tm_own,
+             const __grid_constant__ StepArgs a, const __grid_constant__ FusedDev f, int j) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + F_STAGES * F_STAGE_BYTES);
+    uint64_t* empty = full + F_STAGES;
+    int* slot = reinterpret_cast<int*>(empty + F_STAGES);  // work item of the stage that starts it
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < F_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], F_CONSUMERS / 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const long long g = *a.d_step + j;
+    const int B = a.batch, nz = a.g.nz;
+    const int n_items = f.tiles_x * f.tiles_y * f.n_chunks * B;
+    const int wn = buf_new(g), wc = buf_cur(g), wo = buf_old(g);
+
+    if (tid >= F_CONSUMERS) {
+        // producer: takes work items from the launch's counter and streams
+        // their planes; a stage with item -1 tells the consumers to stop
+        if (tid == F_CONSUMERS) {
+            uint32_t k = 0;
+            bool ok = true;
+            while (ok) {
+                const int s0 = (int)(k % F_STAGES);
+                if (k >= (uint32_t)F_STAGES && !mbar_wait(&empty[s0], ((k / F_STAGES) - 1) & 1)) {
+                    atomicOr(a.flag, 2);
+                    break;
+                }
+                const int item = atomicAdd(f.work + j, 1);
+                if (item >= n_items) {
+                    slot[s0] = -1;
+                    mbar_arrive(&full[s0]);
+                    ++k;
+                    break;
+                }
+                slot[s0] = item;
+                const FusedItem it = fused_item(f, item, nz);
+                const int x0 = it.tx * FT_X, y0 = it.ty * FT_Y;
+                const int zc = (wc * B + it.b) * nz, zo = (wo * B + it.b) * nz;
+                for (int z = it.z0 - 1; z <= it.z1; ++z, ++k) {
+                    const int s = (int)(k % F_STAGES);
+                    if (z > it.z0 - 1 && k >= (uint32_t)F_STAGES &&
+                        !mbar_wait(&empty[s], ((k / F_STAGES) - 1) & 1)) {
+                        ok = false;
+                        atomicOr(a.flag, 2);
+                        break;
+                    }
+                    unsigned char* st = smem + s * F_STAGE_BYTES;
+                    mbar_expect_tx(&full[s], F_TX_BYTES);
+                    tma_load_3d(st, &tm_halo, x0 - 4, y0 - 1, zc + z, &full[s]);
+                    tma_load_3d(st + F_PN_PAD, &tm_own, x0, y0, zo + z, &full[s]);
+                }
+            }
+            // wait for the last copy issued into every stage before leaving
+            for (uint32_t s = 0; s < (uint32_t)F_STAGES && s < k; ++s) {
+                const uint32_t last = k - 1 - ((k - 1 - s) % F_STAGES);
+                mbar_wait(&full[s], (last / F_STAGES) & 1);
+            }
+        }
+        return;
+    }
+
+    const int lane = tid & 31;
+    const int cx = (tid & 15) * 4, cy = tid >> 4;
+    const float L2 = a.lambda2, CI = a.cint;
+    uint32_t k = 0;
+    while (true) {
+        if (!mbar_wait(&full[k % F_STAGES], (k / F_STAGES) & 1)) {
+            if (lane == 0) atomicOr(a.flag, 2);
+            return;
+        }
+        const int item = slot[k % F_STAGES];
+        if (item < 0) break;
+        const FusedItem it = fused_item(f, item, nz);
+        const int x = it.tx * FT_X + cx, y = it.ty * FT_Y + cy;
+        float* pn = a.p[wn] + (size_t)it.b * a.g.vol + (int64_t)y * a.g.pitch + x;
+        const bool yok = (y >= 1 && y <= a.g.ny - 2);
+        const bool xfull = (x >= 1 && x + 3 <= a.g.nx - 2);
+        const int planes = it.z1 - it.z0;
+        if (!mbar_wait(&full[(k + 1) % F_STAGES], ((k + 1) / F_STAGES) & 1)) {
+            if (lane == 0) atomicOr(a.flag, 2);
+            return;
+        }
+        bool bad = false;
+        for (int pl = 0; pl < planes; ++pl) {
+            const int z = it.z0 + pl;
+            const uint32_t kc = k + 1 + pl, kp = kc + 1, km = kc - 1;
+            if (!mbar_wait(&full[kp % F_STAGES], (kp / F_STAGES) & 1)) {
+                if (lane == 0) atomicOr(a.flag, 2);
+                return;
+            }
+            const float* P0 = reinterpret_cast<const float*>(smem + (kc % F_STAGES) * F_STAGE_BYTES);
+            const float* Pm = reinterpret_cast<const float*>(smem + (km % F_STAGES) * F_STAGE_BYTES);
+            const float* Pp = reinterpret_cast<const float*>(smem + (kp % F_STAGES) * F_STAGE_BYTES);
+            const float* O = reinterpret_cast<const float*>(smem + (kc % F_STAGES) * F_STAGE_BYTES + F_PN_PAD);
+            const int s0 = (cy + 1) * FH_X + cx + 4;
+            const float4 c = *reinterpret_cast<const float4*>(P0 + s0);
+            const float xm = P0[s0 - 1], xp = P0[s0 + 4];
+            const float4 ym = *reinterpret_cast<const float4*>(P0 + s0 - FH_X);
+            const float4 yp = *reinterpret_cast<const float4*>(P0 + s0 + FH_X);
+            const float4 zm = *reinterpret_cast<const float4*>(Pm + s0);
+            const float4 zp = *reinterpret_cast<const float4*>(Pp + s0);
+            const float4 o = *reinterpret_cast<const float4*>(O + cy * FT_X + cx);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
+            float4 v;
+            v.x = slf_update(L2, CI, c.y, xm, yp.x, ym.x, zp.x, zm.x, c.x, o.x);
+            v.y = slf_update(L2, CI, c.z, c.x, yp.y, ym.y, zp.y, zm.y, c.y, o.y);
+            v.z = slf_update(L2, CI, c.w, c.y, yp.z, ym.z, zp.z, zm.z, c.z, o.z);
+            v.w = slf_update(L2, CI, xp, c.z, yp.w, ym.w, zp.w, zm.w, c.w, o.w);
+            bad |= !(fabsf(v.x) < 1e30f && fabsf(v.y) < 1e30f && fabsf(v.z) < 1e30f && fabsf(v.w) < 1e30f);
+            if (yok) {
+                float* dst = pn + (int64_t)z * a.g.plane;
+                if (xfull) {
+                    __stcs(reinterpret_cast<float4*>(dst), v);
+                } else {
+                    const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int m = 0; m < 4; ++m)
+                        if (x + m >= 1 && x + m <= a.g.nx - 2) dst[m] = vv[m];
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&empty[(k + planes) % F_STAGES]);
+            mbar_arrive(&empty[(k + planes + 1) % F_STAGES]);
+        }
+        if (__any_sync(0xffffffffu, bad && yok && x <= a.g.nx - 2) && lane == 0) atomicOr(a.flag, 1);
+        k += (uint32_t)planes + 2;
+    }
+}
+
 // source.cl:32-40 then mic.cl:32-41 for one batch member per block.
 // Sources landing on one cell are added in insertion order.
-__global__ void k_src_rcv(StepArgs a, int j) {
+__global__ void k_src_rcv(StepArgs a, int j, int do_src, int do_rcv) {
     const long long g = *a.d_step + j;
     const int b = blockIdx.x;
     float* pn = a.p[buf_new(g)] + (size_t)b * a.g.vol;
-    if (threadIdx.x == 0) {
+    if (do_src && threadIdx.x == 0) {
         for (int s = a.src.begin[b]; s < a.src.begin[b + 1]; ++s) {
             const float v = (g < a.src.len[s]) ? a.src.data[a.src.off[s] + g] : 0.0f;
             pn[a.src.cell[s]] += v;
         }
     }
     __syncthreads();
+    if (!do_rcv) return;
     for (int r = threadIdx.x; r < a.rcv.n; r += blockDim.x) {
         const float v = pn[a.rcv.cell[r]];
         a.rcv.out[((size_t)b * a.rcv.n + r) * a.rcv.cap + g] = v;
@@ -433,6 +643,16 @@ struct Engine::Impl {
     DBuf<int> d_flag;
     DBuf<double> d_energy;
 
+    // fused step plan
+    FusedDev fdev{};
+    DBuf<int4> f_offs;
+    DBuf<int> f_work;
+    CUtensorMap tm_halo{}, tm_own{};
+    int fused_grid = 0;
+    bool fused_dirty = true;
+    std::vector<uint8_t> pml_mask;  // FIXED: slab flags of the PML cells of the grid (host)
+    int tiles_x = 0, tiles_y = 0;
+
     StepArgs args{};
     std::map<int64_t, cudaGraphExec_t> graphs;
     double last_ms = 0.0;
@@ -464,6 +684,12 @@ struct Engine::Impl {
     }
 
     void init_device();
+    void build_fused();
+    bool use_fused() const { return prm.fused != 0; }
+    int64_t tile_key(int x, int y, int z) const {
+        return ((int64_t)(y / FT_Y) * tiles_x + x / FT_X) * nz + z;
+    }
+    static int tile_local(int x, int y) { return (y % FT_Y) * FT_X + x % FT_X; }
     void setup_pml();
     void upload_sources();
     void ensure_receivers(int64_t t_end);
@@ -495,7 +721,22 @@ void Engine::Impl::init_device() {
     CK(cudaSetDevice(device));
     fields.alloc((size_t)vol * 3 * prm.batch);
 
-    // boundary list (in the reference's scan order)
+    tiles_x = (nx + FT_X - 1) / FT_X;
+    tiles_y = (ny + FT_Y - 1) / FT_Y;
+    // boundary list, sorted by (tile, plane, position in tile) for the fused
+    // kernel; the unfused kernel takes any order
+    std::vector<size_t> order(boundary.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t p, size_t q) {
+        const BoundaryPoint &A = boundary[p], &B = boundary[q];
+        const int64_t ka = tile_key(A.x, A.y, A.z), kb = tile_key(B.x, B.y, B.z);
+        if (ka != kb) return ka < kb;
+        return tile_local(A.x, A.y) < tile_local(B.x, B.y);
+    });
+    std::vector<BoundaryPoint> sorted;
+    sorted.reserve(boundary.size());
+    for (size_t k : order) sorted.push_back(boundary[k]);
+    boundary.swap(sorted);
     std::vector<int32_t> cell;
     std::vector<uint32_t> info;
     std::fill(group_counts, group_counts + kNumGroups, 0);
@@ -517,7 +758,57 @@ void Engine::Impl::init_device() {
         coef_a.upload(model.a);
         coef_b.upload(model.b);
     }
+    // tensor maps over the three field levels seen as one stack of
+    // 3 * batch * nz planes: the halo box of p^n and the own box of p^{n-1}
+    {
+        typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                     CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                     CUtensorMapFloatOOBfill);
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) throw Error(AFD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        EncodeFn enc = (EncodeFn)fn;
+        const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)(3 * prm.batch * nz)};
+        const cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)plane * 4};
+        const cuuint32_t box_h[3] = {FH_X, FH_Y, 1}, box_o[3] = {FT_X, FT_Y, 1}, estr[3] = {1, 1, 1};
+        CUresult r1 = enc(&tm_halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, fields.ptr, dims, strides, box_h, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult r2 = enc(&tm_own, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, fields.ptr, dims, strides, box_o, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) throw Error(AFD_ERR_CUDA, "tensor map encoding failed");
+    }
     initialized = true;
+    fused_dirty = true;
+}
+
+// Work decomposition of the streaming kernel: tiles, z-chunk depth and the
+// persistent grid size.
+void Engine::Impl::build_fused() {
+    FusedDev& F = fdev;
+    F = FusedDev{};
+    F.tiles_x = tiles_x;
+    F.tiles_y = tiles_y;
+    int per_sm = 0;
+    CK(cudaFuncSetAttribute((const void*)k_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_stream, F_THREADS, F_SMEM));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int64_t resident = (int64_t)std::max(per_sm, 1) * sms;
+    const int64_t tiles = (int64_t)tiles_x * tiles_y * prm.batch;
+    // z-chunk depth: enough work items for every resident block to take a
+    // few, with the two halo planes a small share of each chunk
+    int dz = 64;
+    while (dz > 8 && tiles * ((nz - 2 + dz - 1) / dz) < 4 * resident) dz /= 2;
+    F.dz = dz;
+    F.n_chunks = (nz - 2 + dz - 1) / dz;
+    if (!f_work.ptr) f_work.alloc(256);
+    F.work = f_work.ptr;
+    fused_grid = (int)std::min<int64_t>(tiles * F.n_chunks, resident);
+    fused_dirty = false;
 }
 
 // SetPml (simulation.hpp:233-277) applied on the device: fresh auxiliary
@@ -532,7 +823,9 @@ void Engine::Impl::setup_pml() {
     psi[1].release();
     pml_cells.release();
     pml_flags.release();
+    pml_mask.clear();
     n_pml_cells = 0;
+    fused_dirty = true;
     pml_g0 = steps_done;
     pml_dirty = false;
     if (pml_width <= 0) return;
@@ -572,9 +865,41 @@ void Engine::Impl::setup_pml() {
                     cells.push_back((int32_t)(z * plane + y * pitch + x));
                     flags.push_back((uint8_t)ax);
                 }
-        pml_cells.upload(cells);
-        pml_flags.upload(flags);
-        n_pml_cells = (int64_t)cells.size();
+        // tile order (spatial locality for the list kernels)
+        std::vector<size_t> order(cells.size());
+        for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+        auto key_of = [&](int32_t c) {
+            const int z = (int)(c / plane), y = (int)((c % plane) / pitch), x = (int)(c % pitch);
+            return std::make_pair(tile_key(x, y, z), tile_local(x, y));
+        };
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t p, size_t q) { return key_of(cells[p]) < key_of(cells[q]); });
+        std::vector<int32_t> c2;
+        std::vector<uint8_t> f2;
+        pml_mask.assign((size_t)nx * ny * nz, 0);
+        for (size_t k = 0; k < cells.size(); ++k) {
+            const int32_t c = cells[k];
+            const int z = (int)(c / plane), y = (int)((c % plane) / pitch), x = (int)(c % pitch);
+            pml_mask[((size_t)z * ny + y) * nx + x] = flags[k];
+        }
+        auto flag_at = [&](int x, int y, int z) -> unsigned {
+            if (x >= nx || y >= ny || z >= nz) return 0u;
+            return pml_mask[((size_t)z * ny + y) * nx + x];
+        };
+        for (size_t k : order) {
+            const int32_t c = cells[k];
+            const int z = (int)(c / plane), y = (int)((c % plane) / pitch), x = (int)(c % pitch);
+            // fields that can be nonzero in the pressure update's reads
+            unsigned rd = 0;
+            for (int dz = 0; dz <= 1; ++dz)
+                for (int dy = 0; dy <= 1; ++dy)
+                    for (int dx = 0; dx <= 1; ++dx) rd |= flag_at(x + dx, y + dy, z + dz);
+            c2.push_back(c);
+            f2.push_back((uint8_t)(flags[k] | (rd << 3)));
+        }
+        pml_cells.upload(c2);
+        pml_flags.upload(f2);
+        n_pml_cells = (int64_t)c2.size();
     }
 }
 
@@ -601,6 +926,7 @@ void Engine::Impl::upload_sources() {
     if (data.empty()) data.push_back(0.0f);
     src_data.upload(data);
     src_dirty = false;
+    fused_dirty = true;
 }
 
 // CheckVariables (simulation.hpp:436-447): the receiver record grows to the
@@ -630,6 +956,7 @@ void Engine::Impl::ensure_receivers(int64_t t_end) {
     rcv_n_dev = nr;
     rcv_cell.upload(cell);
     drop_graphs();
+    fused_dirty = true;
 }
 
 void Engine::Impl::build_args() {
@@ -677,6 +1004,7 @@ void Engine::Impl::build_args() {
     P.inv_dt2 = 1.0f / (dt * dt);
     P.two_dt = 2.0f * dt;
     P.inv_dt = 1.0f / dt;
+    P.psi_on = ref() || ((pml_faces & 3u) && (pml_faces & 12u) && (pml_faces & 48u)) ? 1 : 0;
     a.src.n = (int32_t)src_cell.n;
     a.src.cell = src_cell.ptr;
     a.src.begin = src_begin.ptr;
@@ -690,9 +1018,9 @@ void Engine::Impl::build_args() {
     a.flag = d_flag.ptr;
 }
 
-enum KernelKind { KK_INTERIOR, KK_LRS, KK_PML_AUX, KK_PML_P, KK_SRC_RCV, KK_COUNT };
+enum KernelKind { KK_INTERIOR, KK_LRS, KK_PML_AUX, KK_PML_P, KK_SRC_RCV, KK_FUSED, KK_COUNT };
 static const char* kKernelNames[KK_COUNT] = {"interior", "boundary", "pml_aux", "pml_pressure",
-                                             "source_receiver"};
+                                             "source_receiver", "interior_stream"};
 
 // One time step, global step = *d_step + j (simulation.hpp:358-392).
 void Engine::Impl::launch_step(int j, bool profile) {
@@ -713,7 +1041,12 @@ void Engine::Impl::launch_step(int j, bool profile) {
         CK(cudaEventRecord(ev_pool[ev_kind.size() - 1].second, stream));
     };
     const dim3 blk(64, 4, 1);
-    {
+    if (use_fused()) {
+        begin(KK_FUSED);
+        k_stream<<<fused_grid, F_THREADS, F_SMEM, stream>>>(tm_halo, tm_own, a, fdev, j);
+        end();
+        ++launches;
+    } else {
         const dim3 grd((unsigned)((nx - 2 + 63) / 64), (unsigned)((ny - 2 + 3) / 4),
                        (unsigned)((nz - 2) * prm.batch));
         begin(KK_INTERIOR);
@@ -724,8 +1057,8 @@ void Engine::Impl::launch_step(int j, bool profile) {
     if (a.lrs.n > 0) {
         const dim3 grd((unsigned)((a.lrs.n + 255) / 256), (unsigned)prm.batch);
         begin(KK_LRS);
-        if (ref()) k_lrs<true><<<grd, 256, 0, stream>>>(a, j);
-        else k_lrs<false><<<grd, 256, 0, stream>>>(a, j);
+        if (ref()) launch_lrs<true>(a, j, grd, stream);
+        else launch_lrs<false>(a, j, grd, stream);
         end();
         ++launches;
     }
@@ -755,7 +1088,7 @@ void Engine::Impl::launch_step(int j, bool profile) {
     }
     if (a.src.n > 0 || a.rcv.n > 0) {
         begin(KK_SRC_RCV);
-        k_src_rcv<<<(unsigned)prm.batch, 128, 0, stream>>>(a, j);
+        k_src_rcv<<<(unsigned)prm.batch, 128, 0, stream>>>(a, j, 1, 1);
         end();
         ++launches;
     }
@@ -767,6 +1100,7 @@ cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
     cudaGraph_t graph;
     const int64_t saved = launches;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
     for (int64_t j = 0; j < n; ++j) launch_step((int)j, false);
     k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
     CK(cudaStreamEndCapture(stream, &graph));
@@ -788,6 +1122,7 @@ void Engine::Impl::run_chunk(int64_t n) {
         launch_step_count_only(n);
         (void)before;
     } else {
+        if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
         for (int64_t j = 0; j < n; ++j) launch_step((int)j, profile);
         k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
         ++launches;
@@ -1002,6 +1337,10 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
         D.drop_graphs();
     }
     D.ensure_receivers(D.steps_done + steps);
+    if (D.use_fused() && D.fused_dirty) {
+        D.build_fused();
+        D.drop_graphs();
+    }
     D.build_args();
     D.launches = 0;
     for (auto& st : D.kstats) {
@@ -1029,6 +1368,10 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
             CK(cudaStreamSynchronize(D.stream));
             int flag = 0;
             CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+            if (flag & 2) {
+                D.steps_done += i;
+                throw Error(AFD_ERR_CUDA, "step kernel pipeline wait timed out");
+            }
             if (flag && D.prm.watchdog) {
                 D.steps_done += i;
                 throw Error(AFD_ERR_NUMERIC, "pressure left the finite bound |p| < 1e30 by step " +
@@ -1050,6 +1393,7 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     int flag = 0;
     CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
     D.steps_done += i;
+    if (flag & 2) throw Error(AFD_ERR_CUDA, "step kernel pipeline wait timed out");
     if (flag && D.prm.watchdog)
         throw Error(AFD_ERR_NUMERIC,
                     "pressure left the finite bound |p| < 1e30 by step " + std::to_string(D.steps_done));
