@@ -32,6 +32,14 @@ struct LrsDev {
     float l, l2, c2;  // coefficient l, l*l and 2(1-3*l*l)
 };
 
+// One dense box of PML work (FIXED mode): 4-cell units in x starting at
+// x0, rows y0.., planes z0..; `first` is the running unit count before it.
+struct PmlBox {
+    int32_t x0, units, y0, height, z0, depth;
+    int64_t first;
+};
+constexpr int kMaxPmlBoxes = 6;
+
 // PML state. Full-grid auxiliary fields (two time levels each) per batch
 // member; ksi profiles padded with zeros to kmax entries.
 struct PmlDev {
@@ -41,14 +49,17 @@ struct PmlDev {
     float* fi[3][2];   // [axis][level]
     float* psi[2];
     const float* ksi[3];
-    // FIXED mode: compact list of PML cells with slab flags (bit a = axis a)
-    int32_t n_cells;
-    const int32_t* cells;
-    const uint8_t* flags;
     // scalars, each computed on the host in FP32 exactly as the reference
     // kernel expression would compute it (pml.cl:185-262)
     float dt, cc_dxdx, inv_dx, half_inv_dx, inv_dt2, two_dt, inv_dt;
     int32_t psi_on;    // psi is kept (REF always; FIXED with faces on all three axes)
+    // FIXED mode: disjoint boxes covering the slabs, and a 1-bit mask of the
+    // plain air cells (not solid, not boundary), pitch/32 words per row
+    int32_t n_boxes;
+    PmlBox boxes[kMaxPmlBoxes];
+    int64_t n_units;
+    const uint32_t* air;
+    int32_t words_per_row;
 };
 
 struct SrcDev {
@@ -219,6 +230,60 @@ __device__ __forceinline__ float lrs_point(const LrsDev& L, int e, int b, uint32
             sout[(size_t)slot * n] = 1.0f / a0[f] * (b0[f] * xn + gn[f]);
         }
     }
+    return pn;
+}
+
+// Boundary cell with one solid neighbour in direction d (groups 0-5,
+// lrs_1.cl:61-124): the same arithmetic as lrs_point for one filter, with
+// the neighbour sum and the ring slots resolved without the general
+// pattern handling.
+template <int KT>
+__device__ __forceinline__ float lrs_face(const LrsDev& L, int e, int b, int d, int mat, const float nb[6],
+                                          float pc, float pold, int ix_buf) {
+    const int K = KT > 0 ? KT : L.K;
+    const size_t n = (size_t)L.n;
+    float* sin_ = L.st_in + (size_t)b * L.S * n + e;
+    float* sout = L.st_out + (size_t)b * L.S * n + e;
+    const float* ca = L.ca + mat * K;
+    const float* cb = L.cb + mat * K;
+    const float a0 = __ldg(ca), b0 = __ldg(cb);
+    float gn = 0.0f;
+    auto tap = [&](int i) {
+        int s = ix_buf + i;
+        if (s >= K) s -= K;
+        gn += __ldg(cb + i) * sin_[(size_t)s * n] - __ldg(ca + i) * sout[(size_t)s * n];
+    };
+    if constexpr (KT > 0) {
+#pragma unroll
+        for (int i = 1; i < KT; ++i) tap(i);
+    } else {
+        for (int i = 1; i < K; ++i) tap(i);
+    }
+    // nb: x+1, x-1, y+1, y-1, z+1, z-1; the wall side's term is replaced by
+    // twice the opposite neighbour, axes summed in x, y, z order
+    float S;
+    if (d < 2) {
+        S = 2.0f * nb[d == 0 ? 1 : 0];
+        S = S + nb[2];
+        S = S + nb[3];
+        S = S + nb[4];
+        S = S + nb[5];
+    } else if (d < 4) {
+        S = nb[0] + nb[1];
+        S = S + 2.0f * nb[d == 2 ? 3 : 2];
+        S = S + nb[4];
+        S = S + nb[5];
+    } else {
+        S = nb[0] + nb[1];
+        S = S + nb[2];
+        S = S + nb[3];
+        S = S + 2.0f * nb[d == 4 ? 5 : 4];
+    }
+    const float l = L.l, l2 = L.l2;
+    const float pn = (l2 * S + L.c2 * pc + l2 / b0 * gn + (l * a0 / b0 - 1.0f) * pold) / (1.0f + l * a0 / b0);
+    const float xn = a0 / (l * b0) * (pn - pold) - gn / b0;
+    sin_[(size_t)ix_buf * n] = xn;
+    sout[(size_t)ix_buf * n] = 1.0f / a0 * (b0 * xn + gn);
     return pn;
 }
 

@@ -102,9 +102,15 @@ __global__ void __launch_bounds__(256) k_lrs(const __grid_constant__ StepArgs a,
     const uint32_t info = __ldg(a.lrs.info + e);
     const float nb[6] = {__ldg(pc + c + 1), __ldg(pc + c - 1), __ldg(pc + c + a.g.pitch),
                          __ldg(pc + c - a.g.pitch), __ldg(pc + c + a.g.plane), __ldg(pc + c - a.g.plane)};
-    const float pint = (REF && (info & 31u) == 25u) ? pn[c] : 0.0f;
-    const float v = lrs_point<REF, KT>(a.lrs, e, b, info, nb, __ldg(pc + c), __ldg(po + c), pint,
-                                       ring_index(g, a.lrs.K));
+    const int grp = (int)(info & 31u);
+    const int ix_buf = ring_index(g, a.lrs.K);
+    float v;
+    if (grp < 6) {
+        v = lrs_face<KT>(a.lrs, e, b, grp, (int)((info >> 5) & 255u), nb, __ldg(pc + c), __ldg(po + c), ix_buf);
+    } else {
+        const float pint = (REF && grp == 25) ? pn[c] : 0.0f;
+        v = lrs_point<REF, KT>(a.lrs, e, b, info, nb, __ldg(pc + c), __ldg(po + c), pint, ix_buf);
+    }
     pn[c] = v;
 }
 
@@ -281,102 +287,271 @@ __global__ void __launch_bounds__(256) k_pml_ref_p(StepArgs a, int j) {
     pn[i] = v;
 }
 
-// FIXED pass 1: pressure of the PML cells (pml.cl:185-207 on the PML
-// cells only). An auxiliary field is read only when its slab flags occur in
-// the cell's 2x2x2 cube x..x+1, y..y+1, z..z+1 (bits 3-5 of the flags);
-// elsewhere it is identically zero. psi is kept only when psi_on.
-__global__ void __launch_bounds__(256) k_pml_fix_p(const __grid_constant__ StepArgs a, int j) {
-    const long long g = *a.d_step + j;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.pml.n_cells) return;
-    const int b = blockIdx.y;
-    const size_t base = (size_t)b * a.g.vol;
+// ---- FIXED-mode PML over dense slab boxes ----------------------------------
+// Axes whose enabled slab meets the coordinate ranges (inclusive): for one
+// cell, the auxiliary fields it updates; for a cell's 2x2x2 cube, the fields
+// its pressure update can read as nonzero.
+__device__ __forceinline__ unsigned slab_axes(const StepArgs& a, int x0, int x1, int y0, int y1, int z0,
+                                              int z1) {
+    const uint32_t F = a.pml.faces;
+    const int W = a.pml.width;
+    unsigned ax = 0;
+    if (((F & AFD_FACE_XM) && x0 < W) || ((F & AFD_FACE_XP) && x1 > a.g.nx - W - 1)) ax |= 1u;
+    if (((F & AFD_FACE_YM) && y0 < W) || ((F & AFD_FACE_YP) && y1 > a.g.ny - W - 1)) ax |= 2u;
+    if (((F & AFD_FACE_ZM) && z0 < W) || ((F & AFD_FACE_ZP) && z1 > a.g.nz - W - 1)) ax |= 4u;
+    return ax;
+}
+
+// The four cells x..x+3 of row (y, z) that are PML cells (inside 2..n-3,
+// in an enabled slab, plain air), as a bit mask.
+__device__ __forceinline__ unsigned pml_mask4(const StepArgs& a, int x, int y, int z) {
     const PmlDev& P = a.pml;
+    const uint32_t w =
+        (__ldg(P.air + ((int64_t)z * a.g.ny + y) * P.words_per_row + (x >> 5)) >> (x & 31)) & 15u;
+    unsigned m = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int xx = x + q;
+        if (((w >> q) & 1u) && xx >= 2 && xx <= a.g.nx - 3 && slab_axes(a, xx, xx, y, y, z, z)) m |= 1u << q;
+    }
+    return m;
+}
+
+// Thread -> (batch member, first cell) of a box launch: x in 4-cell units,
+// rows in y, planes (times batch members) in z.
+__device__ __forceinline__ bool box_cell(const PmlBox& bx, int& b, int& x, int& y, int& z) {
+    const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+    const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ux >= bx.units || yy >= bx.height) return false;
+    b = (int)(blockIdx.z / (unsigned)bx.depth);
+    z = bx.z0 + (int)(blockIdx.z % (unsigned)bx.depth);
+    x = bx.x0 + 4 * ux;
+    y = bx.y0 + yy;
+    return true;
+}
+
+__device__ __forceinline__ void row5(const float* p, float r[5]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    r[0] = v.x;
+    r[1] = v.y;
+    r[2] = v.z;
+    r[3] = v.w;
+    r[4] = __ldg(p + 4);
+}
+
+__device__ __forceinline__ void store4(float* p, const float v[4], unsigned m) {
+    if (m == 15u) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (m & (1u << q)) p[q] = v[q];
+    }
+}
+
+// Pressure of the PML cells (pml.cl:185-207 restricted to the slab cells)
+// over one box of the disjoint box cover, four consecutive cells per
+// thread. Fields outside the read axes are identically zero there and are
+// not loaded; PSI: psi is kept (PML faces on all three axes).
+template <bool PSI>
+__global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepArgs a, const PmlBox bx, int j) {
+    int b, x, y, z;
+    if (!box_cell(bx, b, x, y, z)) return;
+    const unsigned m = pml_mask4(a, x, y, z);
+    if (!m) return;
+    const PmlDev& P = a.pml;
+    const long long g = *a.d_step + j;
+    const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
-    float* pn = a.p[buf_new(g)] + base;
+    const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
     const float* pc = a.p[buf_cur(g)] + base;
     const float* po = a.p[buf_old(g)] + base;
+    float* pn = a.p[buf_new(g)] + base;
     const int lv = pml_level(a, g);
-    const int64_t i = __ldg(P.cells + e);
-    const unsigned axes = __ldg(P.flags + e) >> 3;
-    const int z = (int)(i / plane);
-    const int y = (int)((i % plane) / pitch);
-    const int x = (int)(i % pitch);
-    const float kx = __ldg(P.ksi[0] + x), ky = __ldg(P.ksi[1] + y), kz = __ldg(P.ksi[2] + z);
-    const float pm1 = __ldg(pc + i), pm2 = __ldg(po + i);
-    float ps = 0.0f, pmh = 0.0f;
-    if (P.psi_on) {
-        pmh = P.psi[lv ^ 1][base + i];
-        ps = P.dt * pm1 + pmh;
-        P.psi[lv][base + i] = ps;
+    float c[5], ym4[5], yp4[5], zm4[5], zp4[5], o[5];
+    row5(pc + i, c);
+    const float xm = __ldg(pc + i - 1);
+    row5(pc + i - pitch, ym4);
+    row5(pc + i + pitch, yp4);
+    row5(pc + i - plane, zm4);
+    row5(pc + i + plane, zp4);
+    row5(po + i, o);
+    const float4 kx4 = __ldg(reinterpret_cast<const float4*>(P.ksi[0] + x));
+    const float kxv[4] = {kx4.x, kx4.y, kx4.z, kx4.w};
+    const float ky = __ldg(P.ksi[1] + y), kz = __ldg(P.ksi[2] + z);
+    const unsigned ra = slab_axes(a, x, x + 4, y, y + 1, z, z + 1);
+    float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (ra & 1u) {
+        const float* f = P.fi[0][lv ^ 1] + base + i;
+        float r00[5], r01[5], r10[5], r11[5], av[5];
+        row5(f, r00);
+        row5(f + plane, r01);
+        row5(f + pitch, r10);
+        row5(f + pitch + plane, r11);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) av[q] = 0.25f * (((r00[q] + r01[q]) + r10[q]) + r11[q]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = av[q + 1] - av[q];
     }
-    float s = __ldg(pc + i + 1) + __ldg(pc + i - 1);
-    s = s + __ldg(pc + i + pitch);
-    s = s + __ldg(pc + i - pitch);
-    s = s + __ldg(pc + i + plane);
-    s = s + __ldg(pc + i - plane);
-    s = s - 6.0f * pm1;
-    const float A = P.cc_dxdx * s;
-    float d = 0.0f;
-    if (axes & 1u) {
-        const float* f = P.fi[0][lv ^ 1] + base;
-        const float a1 = 0.25f * (((__ldg(f + i + 1) + __ldg(f + i + 1 + plane)) + __ldg(f + i + 1 + pitch)) +
-                                  __ldg(f + i + 1 + pitch + plane));
-        const float a0 = 0.25f * (((__ldg(f + i) + __ldg(f + i + plane)) + __ldg(f + i + pitch)) +
-                                  __ldg(f + i + pitch + plane));
-        d = a1 - a0;
+    if (ra & 2u) {
+        const float* f = P.fi[1][lv ^ 1] + base + i;
+        float r00[5], r01[5], r10[5], r11[5];
+        row5(f, r00);
+        row5(f + plane, r01);
+        row5(f + pitch, r10);
+        row5(f + pitch + plane, r11);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float a1 = 0.25f * (((r10[q] + r11[q]) + r10[q + 1]) + r11[q + 1]);
+            const float a0 = 0.25f * (((r00[q] + r01[q]) + r00[q + 1]) + r01[q + 1]);
+            d[q] = d[q] + a1;
+            d[q] = d[q] - a0;
+        }
     }
-    if (axes & 2u) {
-        const float* f = P.fi[1][lv ^ 1] + base;
-        const int64_t q = i + pitch;
-        const float a1 = 0.25f * (((__ldg(f + q) + __ldg(f + q + plane)) + __ldg(f + q + 1)) + __ldg(f + q + 1 + plane));
-        const float a0 = 0.25f * (((__ldg(f + i) + __ldg(f + i + plane)) + __ldg(f + i + 1)) + __ldg(f + i + 1 + plane));
-        d = d + a1;
-        d = d - a0;
+    if (ra & 4u) {
+        const float* f = P.fi[2][lv ^ 1] + base + i;
+        float r00[5], r01[5], r10[5], r11[5];
+        row5(f, r00);
+        row5(f + plane, r01);
+        row5(f + pitch, r10);
+        row5(f + pitch + plane, r11);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float a1 = 0.25f * (((r01[q] + r11[q]) + r01[q + 1]) + r11[q + 1]);
+            const float a0 = 0.25f * (((r00[q] + r10[q]) + r00[q + 1]) + r10[q + 1]);
+            d[q] = d[q] + a1;
+            d[q] = d[q] - a0;
+        }
     }
-    if (axes & 4u) {
-        const float* f = P.fi[2][lv ^ 1] + base;
-        const int64_t q = i + plane;
-        const float a1 = 0.25f * (((__ldg(f + q) + __ldg(f + q + pitch)) + __ldg(f + q + 1)) + __ldg(f + q + 1 + pitch));
-        const float a0 = 0.25f * (((__ldg(f + i) + __ldg(f + i + pitch)) + __ldg(f + i + 1)) + __ldg(f + i + 1 + pitch));
-        d = d + a1;
-        d = d - a0;
+    float ps[4] = {0.0f, 0.0f, 0.0f, 0.0f}, pmh[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (PSI) {
+        const float4 h = *reinterpret_cast<const float4*>(P.psi[lv ^ 1] + base + i);
+        pmh[0] = h.x;
+        pmh[1] = h.y;
+        pmh[2] = h.z;
+        pmh[3] = h.w;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ps[q] = P.dt * c[q] + pmh[q];
+        store4(P.psi[lv] + base + i, ps, m);
     }
-    const float B = P.inv_dx * d;
-    const float C = kx * ky * kz * 0.5f * (ps + pmh);
-    const float D = P.inv_dt2 * (pm2 - 2.0f * pm1);
-    const float E = (kx * ky + ky * kz + kz * kx) * pm1;
-    const float F = (kx + ky + kz) / P.two_dt * pm2;
-    const float num = A + B - C - D - E + F;
-    const float v = num / (P.inv_dt2 + (kx + ky + kz) / P.two_dt);
-    pn[i] = v;
-    watch(a.flag, v);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float xmq = q == 0 ? xm : c[q - 1];
+        float s6 = c[q + 1] + xmq;
+        s6 = s6 + yp4[q];
+        s6 = s6 + ym4[q];
+        s6 = s6 + zp4[q];
+        s6 = s6 + zm4[q];
+        const float kx = kxv[q];
+        const float ks = (kx + ky + kz) / P.two_dt;
+        const float A = P.cc_dxdx * (s6 - 6.0f * c[q]);
+        const float B = P.inv_dx * d[q];
+        const float C = kx * ky * kz * 0.5f * (ps[q] + pmh[q]);
+        const float D = P.inv_dt2 * (o[q] - 2.0f * c[q]);
+        const float E = (kx * ky + ky * kz + kz * kx) * c[q];
+        const float F = ks * o[q];
+        const float num = A + B - C - D - E + F;
+        v[q] = num / (P.inv_dt2 + ks);
+        if ((m >> q) & 1u) watch(a.flag, v[q]);
+    }
+    store4(pn + i, v, m);
 }
 
-// FIXED pass 2: auxiliary fields from the complete new pressure and psi.
-__global__ void __launch_bounds__(256) k_pml_fix_aux(const __grid_constant__ StepArgs a, int j) {
+// Auxiliary field AX of the PML cells of one slab box (pml.cl:231-262 with
+// the derivative and ksi index corrected). The derivatives of the new and
+// previous pressure along every axis come from the same four rows
+// (y, y+1) x (z, z+1), x..x+4.
+template <int AX, bool PSI>
+__global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ StepArgs a, const PmlBox bx,
+                                                     int j) {
+    int b, x, y, z;
+    if (!box_cell(bx, b, x, y, z)) return;
+    const unsigned m = pml_mask4(a, x, y, z);
+    if (!m) return;
+    const PmlDev& P = a.pml;
     const long long g = *a.d_step + j;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.pml.n_cells) return;
-    const unsigned axes = __ldg(a.pml.flags + e) & 7u;
-    if (!axes) return;
-    const int b = blockIdx.y;
     const size_t base = (size_t)b * a.g.vol;
-    const float* pn = a.p[buf_new(g)] + base;
-    const float* pc = a.p[buf_cur(g)] + base;
+    const int64_t pitch = a.g.pitch, plane = a.g.plane;
+    const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
+    const float* pn = a.p[buf_new(g)] + base + i;
+    const float* pc = a.p[buf_cur(g)] + base + i;
     const int lv = pml_level(a, g);
-    const int64_t i = a.pml.cells[e];
-    const int z = (int)(i / a.g.plane);
-    const int y = (int)((i % a.g.plane) / a.g.pitch);
-    const int x = (int)(i % a.g.pitch);
-    pml_aux<false>(a, axes, pn, pc, a.pml.psi[lv] + base, 0.0f, 0.0f, a.pml.fi[0][lv ^ 1] + base,
-                   a.pml.fi[1][lv ^ 1] + base, a.pml.fi[2][lv ^ 1] + base, a.pml.fi[0][lv] + base,
-                   a.pml.fi[1][lv] + base, a.pml.fi[2][lv] + base, x, y, z, i);
+    float n00[5], n01[5], n10[5], n11[5], m00[5], m01[5], m10[5], m11[5];
+    row5(pn, n00);
+    row5(pn + plane, n01);
+    row5(pn + pitch, n10);
+    row5(pn + pitch + plane, n11);
+    row5(pc, m00);
+    row5(pc + plane, m01);
+    row5(pc + pitch, m10);
+    row5(pc + pitch + plane, m11);
+    float s00[5] = {0}, s01[5] = {0}, s10[5] = {0}, s11[5] = {0};
+    if (PSI) {
+        const float* ps = P.psi[lv] + base + i;
+        row5(ps, s00);
+        row5(ps + plane, s01);
+        row5(ps + pitch, s10);
+        row5(ps + pitch + plane, s11);
+    }
+    float kxs[5];
+    row5(P.ksi[0] + x, kxs);
+    const float kay = 0.5f * (__ldg(P.ksi[1] + y) + __ldg(P.ksi[1] + y + 1));
+    const float kaz = 0.5f * (__ldg(P.ksi[2] + z) + __ldg(P.ksi[2] + z + 1));
+    const float4 f14 = *reinterpret_cast<const float4*>(P.fi[AX][lv ^ 1] + base + i);
+    const float f1v[4] = {f14.x, f14.y, f14.z, f14.w};
+    float out[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float kax = 0.5f * (kxs[q] + kxs[q + 1]);
+        const float f1 = f1v[q];
+        if (AX == 0) {
+            const float an1 = 0.25f * (((n00[q + 1] + n01[q + 1]) + n10[q + 1]) + n11[q + 1]);
+            const float an0 = 0.25f * (((n00[q] + n01[q]) + n10[q]) + n11[q]);
+            const float am1 = 0.25f * (((m00[q + 1] + m01[q + 1]) + m10[q + 1]) + m11[q + 1]);
+            const float am0 = 0.25f * (((m00[q] + m01[q]) + m10[q]) + m11[q]);
+            const float dxp = P.half_inv_dx * (an1 - an0 + am1 - am0);
+            float dxpsi = 0.0f;
+            if (PSI) {
+                const float as1 = 0.25f * (((s00[q + 1] + s01[q + 1]) + s10[q + 1]) + s11[q + 1]);
+                const float as0 = 0.25f * (((s00[q] + s01[q]) + s10[q]) + s11[q]);
+                dxpsi = P.inv_dx * (as1 - as0);
+            }
+            out[q] = (-0.5f * kax * f1 + (kay + kaz - kax) * dxp + (kay * kaz) * dxpsi + P.inv_dt * f1) /
+                     (P.inv_dt + kax * 0.5f);
+        } else if (AX == 1) {
+            const float an1 = 0.25f * (((n10[q] + n11[q]) + n10[q + 1]) + n11[q + 1]);
+            const float an0 = 0.25f * (((n00[q] + n01[q]) + n00[q + 1]) + n01[q + 1]);
+            const float am1 = 0.25f * (((m10[q] + m11[q]) + m10[q + 1]) + m11[q + 1]);
+            const float am0 = 0.25f * (((m00[q] + m01[q]) + m00[q + 1]) + m01[q + 1]);
+            const float dyp = P.half_inv_dx * (an1 - an0 + am1 - am0);
+            float dypsi = 0.0f;
+            if (PSI) {
+                const float as1 = 0.25f * (((s10[q] + s11[q]) + s10[q + 1]) + s11[q + 1]);
+                const float as0 = 0.25f * (((s00[q] + s01[q]) + s00[q + 1]) + s01[q + 1]);
+                dypsi = P.inv_dx * (as1 - as0);
+            }
+            out[q] = (-0.5f * kay * f1 + (kax + kaz - kay) * dyp + (kax * kaz) * dypsi + P.inv_dt * f1) /
+                     (P.inv_dt + kay * 0.5f);
+        } else {
+            const float an1 = 0.25f * (((n01[q] + n11[q]) + n01[q + 1]) + n11[q + 1]);
+            const float an0 = 0.25f * (((n00[q] + n10[q]) + n00[q + 1]) + n10[q + 1]);
+            const float am1 = 0.25f * (((m01[q] + m11[q]) + m01[q + 1]) + m11[q + 1]);
+            const float am0 = 0.25f * (((m00[q] + m10[q]) + m00[q + 1]) + m10[q + 1]);
+            const float dzp = P.half_inv_dx * (an1 - an0 + am1 - am0);
+            float dzpsi = 0.0f;
+            if (PSI) {
+                const float as1 = 0.25f * (((s01[q] + s11[q]) + s01[q + 1]) + s11[q + 1]);
+                const float as0 = 0.25f * (((s00[q] + s10[q]) + s00[q + 1]) + s10[q + 1]);
+                dzpsi = P.inv_dx * (as1 - as0);
+            }
+            out[q] = (-0.5f * kaz * f1 + (kax + kay - kaz) * dzp + (kax * kay) * dzpsi + P.inv_dt * f1) /
+                     (P.inv_dt + kaz * 0.5f);
+        }
+    }
+    store4(P.fi[AX][lv] + base + i, out, m);
 }
 
-// ---------------------------------------------------------------------------
-// Fused step kernel (see fused.cuh for the structure)
-// ---------------------------------------------------------------------------
 // Interior SLF update of every cell 1..n-2 (leapfrog.cl:34-55) streamed
 // through shared memory; see fused.cuh. Consumer warps wait on the stage
 // barriers independently (no block-wide barrier), so a slow warp delays
@@ -541,6 +716,38 @@ __global__ void k_src_rcv(StepArgs a, int j, int do_src, int do_rcv) {
     }
 }
 
+// Sources and receivers with their cells passed as kernel parameters (no
+// dependent metadata loads): source.cl:32-40 then mic.cl:32-41.
+constexpr int kInlineSrc = 64, kInlineRcv = 256;
+struct SrcRcvInline {
+    int32_t n_src, n_rcv;
+    int32_t src_cell[kInlineSrc];
+    int32_t src_batch[kInlineSrc];
+    int64_t src_len[kInlineSrc];
+    const float* src_ptr[kInlineSrc];
+    int32_t rcv_cell[kInlineRcv];
+};
+
+__global__ void k_src_rcv_inline(const __grid_constant__ StepArgs a, const __grid_constant__ SrcRcvInline q,
+                                 int j) {
+    const long long g = *a.d_step + j;
+    const int b = blockIdx.x;
+    float* pn = a.p[buf_new(g)] + (size_t)b * a.g.vol;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < q.n_src; ++s) {
+            if (q.src_batch[s] != b) continue;
+            const float v = (g < q.src_len[s]) ? __ldg(q.src_ptr[s] + g) : 0.0f;
+            pn[q.src_cell[s]] += v;
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < q.n_rcv; r += blockDim.x) {
+        const float v = pn[q.rcv_cell[r]];
+        a.rcv.out[((size_t)b * q.n_rcv + r) * a.rcv.cap + g] = v;
+        watch(a.flag, v);
+    }
+}
+
 __global__ void k_advance(long long* d_step, int n) { *d_step += n; }
 
 // Discrete SLF energy between the two latest levels u1 (newest) and u0,
@@ -629,8 +836,10 @@ struct Engine::Impl {
     DBuf<float> coef_a, coef_b;
     DBuf<float> fi[3][2], psi[2];
     DBuf<float> ksi_dev[3];
-    DBuf<int32_t> pml_cells;
-    DBuf<uint8_t> pml_flags;
+    DBuf<uint32_t> pml_air;
+    std::vector<PmlBox> pml_boxes;
+    std::vector<PmlBox> pml_axis_boxes[3];
+    int64_t pml_units = 0;
     int64_t n_pml_cells = 0;
     DBuf<int32_t> src_cell, src_begin;
     DBuf<int64_t> src_off, src_len;
@@ -650,10 +859,11 @@ struct Engine::Impl {
     CUtensorMap tm_halo{}, tm_own{};
     int fused_grid = 0;
     bool fused_dirty = true;
-    std::vector<uint8_t> pml_mask;  // FIXED: slab flags of the PML cells of the grid (host)
     int tiles_x = 0, tiles_y = 0;
 
     StepArgs args{};
+    SrcRcvInline inl{};
+    bool inline_ok = false;
     std::map<int64_t, cudaGraphExec_t> graphs;
     double last_ms = 0.0;
     int64_t launches = 0;
@@ -821,9 +1031,10 @@ void Engine::Impl::setup_pml() {
     }
     psi[0].release();
     psi[1].release();
-    pml_cells.release();
-    pml_flags.release();
-    pml_mask.clear();
+    pml_air.release();
+    pml_boxes.clear();
+    for (auto& v : pml_axis_boxes) v.clear();
+    pml_units = 0;
     n_pml_cells = 0;
     fused_dirty = true;
     pml_g0 = steps_done;
@@ -834,7 +1045,7 @@ void Engine::Impl::setup_pml() {
     psi[0].alloc((size_t)vol * prm.batch);
     psi[1].alloc((size_t)vol * prm.batch);
     // padded so that the reference's ksi_x[y] read (pml.cl:247) stays in bounds
-    const int32_t kmax = std::max(nx, std::max(ny, nz)) + 1;
+    const int32_t kmax = std::max(nx, std::max(ny, nz)) + 8;
     const int32_t dims[3] = {nx, ny, nz};
     for (int a = 0; a < 3; ++a) {
         std::vector<float> k((size_t)kmax, 0.0f);
@@ -842,64 +1053,106 @@ void Engine::Impl::setup_pml() {
         ksi_dev[a].upload(k);
     }
     if (!ref()) {
-        // FIXED: non-boundary air cells 2..n-3 inside an enabled face slab
-        std::vector<uint8_t> is_lrs((size_t)nx * ny * nz, 0);
-        for (const BoundaryPoint& b : boundary) is_lrs[((size_t)b.z * ny + b.y) * nx + b.x] = 1;
+        // FIXED: PML cells are the plain air cells (not solid, not boundary)
+        // with 2 <= x, y, z <= n-3 inside an enabled face slab. The kernels
+        // walk disjoint boxes covering the slabs and test a 1-bit air mask.
         const int W = pml_width;
-        std::vector<int32_t> cells;
-        std::vector<uint8_t> flags;
-        for (int z = 2; z <= nz - 3; ++z)
-            for (int y = 2; y <= ny - 3; ++y)
-                for (int x = 2; x <= nx - 3; ++x) {
-                    unsigned ax = 0;
-                    if (((pml_faces & AFD_FACE_XM) && x < W) || ((pml_faces & AFD_FACE_XP) && x > nx - W - 1))
-                        ax |= 1u;
-                    if (((pml_faces & AFD_FACE_YM) && y < W) || ((pml_faces & AFD_FACE_YP) && y > ny - W - 1))
-                        ax |= 2u;
-                    if (((pml_faces & AFD_FACE_ZM) && z < W) || ((pml_faces & AFD_FACE_ZP) && z > nz - W - 1))
-                        ax |= 4u;
-                    if (!ax) continue;
-                    if (is_lrs[((size_t)z * ny + y) * nx + x]) continue;
+        const uint32_t F = pml_faces;
+        const int wpr = (int)(pitch / 32);
+        std::vector<uint8_t> is_lrs((size_t)nx * ny * nz, 0);
+        for (const BoundaryPoint& bp : boundary) is_lrs[((size_t)bp.z * ny + bp.y) * nx + bp.x] = 1;
+        std::vector<uint32_t> air((size_t)nz * ny * wpr, 0u);
+        auto in_slab = [&](int x, int y, int z) {
+            return ((F & AFD_FACE_XM) && x < W) || ((F & AFD_FACE_XP) && x > nx - W - 1) ||
+                   ((F & AFD_FACE_YM) && y < W) || ((F & AFD_FACE_YP) && y > ny - W - 1) ||
+                   ((F & AFD_FACE_ZM) && z < W) || ((F & AFD_FACE_ZP) && z > nz - W - 1);
+        };
+        int64_t npml = 0;
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    const size_t c = ((size_t)z * ny + y) * nx + x;
+                    if (is_lrs[c]) continue;
                     if (have_model && x < model.nx && y < model.ny && z < model.nz && model.at(x, y, z) != -1)
                         continue;
-                    cells.push_back((int32_t)(z * plane + y * pitch + x));
-                    flags.push_back((uint8_t)ax);
+                    air[((size_t)z * ny + y) * wpr + (x >> 5)] |= 1u << (x & 31);
+                    if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3 && z >= 2 && z <= nz - 3 && in_slab(x, y, z))
+                        ++npml;
                 }
-        // tile order (spatial locality for the list kernels)
-        std::vector<size_t> order(cells.size());
-        for (size_t k = 0; k < order.size(); ++k) order[k] = k;
-        auto key_of = [&](int32_t c) {
-            const int z = (int)(c / plane), y = (int)((c % plane) / pitch), x = (int)(c % pitch);
-            return std::make_pair(tile_key(x, y, z), tile_local(x, y));
+        n_pml_cells = npml;
+        pml_air.upload(air);
+        // disjoint boxes: z slabs take whole planes, y slabs the remaining
+        // planes, x slabs the remaining rows
+        pml_boxes.clear();
+        auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
+            if (x0 > x1 || y0 > y1 || z0 > z1) return;
+            PmlBox bx{};
+            bx.x0 = x0 & ~3;
+            bx.units = (x1 - bx.x0) / 4 + 1;
+            bx.y0 = y0;
+            bx.height = y1 - y0 + 1;
+            bx.z0 = z0;
+            bx.depth = z1 - z0 + 1;
+            pml_boxes.push_back(bx);
         };
-        std::stable_sort(order.begin(), order.end(),
-                         [&](size_t p, size_t q) { return key_of(cells[p]) < key_of(cells[q]); });
-        std::vector<int32_t> c2;
-        std::vector<uint8_t> f2;
-        pml_mask.assign((size_t)nx * ny * nz, 0);
-        for (size_t k = 0; k < cells.size(); ++k) {
-            const int32_t c = cells[k];
-            const int z = (int)(c / plane), y = (int)((c % plane) / pitch), x = (int)(c % pitch);
-            pml_mask[((size_t)z * ny + y) * nx + x] = flags[k];
+        int lo[3] = {2, 2, 2}, hi[3] = {nx - 3, ny - 3, nz - 3};
+        const int dims3[3] = {nx, ny, nz};
+        int rest_lo[3] = {2, 2, 2}, rest_hi[3] = {nx - 3, ny - 3, nz - 3};
+        for (int ax = 2; ax >= 0; --ax) {
+            const bool m_face = F & (1u << (2 * ax)), p_face = F & (2u << (2 * ax));
+            int mlo = lo[ax], mhi = std::min(W - 1, hi[ax]);
+            int plo = std::max(dims3[ax] - W, lo[ax]), phi = hi[ax];
+            if (m_face && p_face && plo <= mhi) plo = mhi + 1;
+            int box_lo[3], box_hi[3];
+            for (int k = 0; k < 3; ++k) {
+                box_lo[k] = k > ax ? rest_lo[k] : lo[k];
+                box_hi[k] = k > ax ? rest_hi[k] : hi[k];
+            }
+            if (m_face) {
+                box_lo[ax] = mlo;
+                box_hi[ax] = mhi;
+                add(box_lo[0], box_hi[0], box_lo[1], box_hi[1], box_lo[2], box_hi[2]);
+                rest_lo[ax] = std::max(rest_lo[ax], mhi + 1);
+            }
+            if (p_face) {
+                box_lo[ax] = plo;
+                box_hi[ax] = phi;
+                add(box_lo[0], box_hi[0], box_lo[1], box_hi[1], box_lo[2], box_hi[2]);
+                rest_hi[ax] = std::min(rest_hi[ax], plo - 1);
+            }
         }
-        auto flag_at = [&](int x, int y, int z) -> unsigned {
-            if (x >= nx || y >= ny || z >= nz) return 0u;
-            return pml_mask[((size_t)z * ny + y) * nx + x];
-        };
-        for (size_t k : order) {
-            const int32_t c = cells[k];
-            const int z = (int)(c / plane), y = (int)((c % plane) / pitch), x = (int)(c % pitch);
-            // fields that can be nonzero in the pressure update's reads
-            unsigned rd = 0;
-            for (int dz = 0; dz <= 1; ++dz)
-                for (int dy = 0; dy <= 1; ++dy)
-                    for (int dx = 0; dx <= 1; ++dx) rd |= flag_at(x + dx, y + dy, z + dz);
-            c2.push_back(c);
-            f2.push_back((uint8_t)(flags[k] | (rd << 3)));
+        int64_t first = 0;
+        for (PmlBox& bx : pml_boxes) {
+            bx.first = first;
+            first += (int64_t)bx.units * bx.height * bx.depth;
         }
-        pml_cells.upload(c2);
-        pml_flags.upload(f2);
-        n_pml_cells = (int64_t)c2.size();
+        pml_units = first;
+        // per-axis slab boxes for the auxiliary fields (a cell in two slabs
+        // updates one field in each)
+        for (int ax = 0; ax < 3; ++ax) {
+            pml_axis_boxes[ax].clear();
+            const bool m_face = F & (1u << (2 * ax)), p_face = F & (2u << (2 * ax));
+            const int mhi = std::min(W - 1, hi[ax]);
+            int plo = std::max(dims3[ax] - W, lo[ax]);
+            if (m_face && p_face && plo <= mhi) plo = mhi + 1;
+            auto push = [&](int alo, int ahi) {
+                int l3[3] = {lo[0], lo[1], lo[2]}, h3[3] = {hi[0], hi[1], hi[2]};
+                l3[ax] = alo;
+                h3[ax] = ahi;
+                if (l3[0] > h3[0] || l3[1] > h3[1] || l3[2] > h3[2]) return;
+                PmlBox bx{};
+                bx.x0 = l3[0] & ~3;
+                bx.units = (h3[0] - bx.x0) / 4 + 1;
+                bx.y0 = l3[1];
+                bx.height = h3[1] - l3[1] + 1;
+                bx.z0 = l3[2];
+                bx.depth = h3[2] - l3[2] + 1;
+                pml_axis_boxes[ax].push_back(bx);
+            };
+            if (m_face) push(lo[ax], mhi);
+            if (p_face) push(plo, hi[ax]);
+        }
+        if ((int)pml_boxes.size() > kMaxPmlBoxes) throw Error(AFD_ERR_ARG, "too many PML boxes");
     }
 }
 
@@ -993,9 +1246,6 @@ void Engine::Impl::build_args() {
     }
     P.psi[0] = psi[0].ptr;
     P.psi[1] = psi[1].ptr;
-    P.n_cells = (int32_t)n_pml_cells;
-    P.cells = pml_cells.ptr;
-    P.flags = pml_flags.ptr;
     const float c = prm.c, dx = prm.dx, dt = prm.dt;
     P.dt = dt;
     P.cc_dxdx = c * c / (dx * dx);
@@ -1005,6 +1255,11 @@ void Engine::Impl::build_args() {
     P.two_dt = 2.0f * dt;
     P.inv_dt = 1.0f / dt;
     P.psi_on = ref() || ((pml_faces & 3u) && (pml_faces & 12u) && (pml_faces & 48u)) ? 1 : 0;
+    P.n_boxes = (int32_t)pml_boxes.size();
+    for (size_t k = 0; k < pml_boxes.size(); ++k) P.boxes[k] = pml_boxes[k];
+    P.n_units = pml_units;
+    P.air = pml_air.ptr;
+    P.words_per_row = (int32_t)(pitch / 32);
     a.src.n = (int32_t)src_cell.n;
     a.src.cell = src_cell.ptr;
     a.src.begin = src_begin.ptr;
@@ -1016,6 +1271,27 @@ void Engine::Impl::build_args() {
     a.rcv.out = rcv_out.ptr;
     a.rcv.cap = rcv_cap;
     a.flag = d_flag.ptr;
+    // inline source/receiver table (device order of upload_sources)
+    inline_ok = (int64_t)sources.size() <= kInlineSrc && (int64_t)receivers.size() <= kInlineRcv;
+    inl = SrcRcvInline{};
+    if (inline_ok) {
+        int64_t off = 0;
+        int k = 0;
+        for (int32_t bm = 0; bm < prm.batch; ++bm)
+            for (const Source& q : sources) {
+                if (q.batch != bm) continue;
+                inl.src_cell[k] = (int32_t)(q.ijk[2] * plane + q.ijk[1] * pitch + q.ijk[0]);
+                inl.src_batch[k] = bm;
+                inl.src_len[k] = (int64_t)q.sig.size();
+                inl.src_ptr[k] = src_data.ptr + off;
+                off += (int64_t)q.sig.size();
+                ++k;
+            }
+        inl.n_src = k;
+        inl.n_rcv = (int32_t)receivers.size();
+        for (size_t r = 0; r < receivers.size(); ++r)
+            inl.rcv_cell[r] = (int32_t)(receivers[r][2] * plane + receivers[r][1] * pitch + receivers[r][0]);
+    }
 }
 
 enum KernelKind { KK_INTERIOR, KK_LRS, KK_PML_AUX, KK_PML_P, KK_SRC_RCV, KK_FUSED, KK_COUNT };
@@ -1075,20 +1351,48 @@ void Engine::Impl::launch_step(int j, bool profile) {
                 end();
                 launches += 2;
             }
-        } else if (a.pml.n_cells > 0) {
-            const dim3 grd((unsigned)((a.pml.n_cells + 255) / 256), (unsigned)prm.batch);
-            begin(KK_PML_P);
-            k_pml_fix_p<<<grd, 256, 0, stream>>>(a, j);
-            end();
-            begin(KK_PML_AUX);
-            k_pml_fix_aux<<<grd, 256, 0, stream>>>(a, j);
-            end();
-            launches += 2;
+        } else if (a.pml.n_units > 0) {
+            auto shape = [&](const PmlBox& bx, dim3& grd, dim3& blk) {
+                unsigned w = 1;
+                while ((int)w < bx.units && w < 32) w <<= 1;
+                blk = dim3(w, 256 / w, 1);
+                grd = dim3((unsigned)((bx.units + w - 1) / w), (unsigned)((bx.height + blk.y - 1) / blk.y),
+                           (unsigned)(bx.depth * prm.batch));
+            };
+            const bool psi = a.pml.psi_on != 0;
+            for (const PmlBox& bx : pml_boxes) {
+                dim3 grd, blk;
+                shape(bx, grd, blk);
+                begin(KK_PML_P);
+                if (psi) k_pml_box_p<true><<<grd, blk, 0, stream>>>(a, bx, j);
+                else k_pml_box_p<false><<<grd, blk, 0, stream>>>(a, bx, j);
+                end();
+                ++launches;
+            }
+            for (int ax = 0; ax < 3; ++ax)
+                for (const PmlBox& bx : pml_axis_boxes[ax]) {
+                    dim3 grd, blk;
+                    shape(bx, grd, blk);
+                    begin(KK_PML_AUX);
+                    if (ax == 0) {
+                        if (psi) k_pml_box_aux<0, true><<<grd, blk, 0, stream>>>(a, bx, j);
+                        else k_pml_box_aux<0, false><<<grd, blk, 0, stream>>>(a, bx, j);
+                    } else if (ax == 1) {
+                        if (psi) k_pml_box_aux<1, true><<<grd, blk, 0, stream>>>(a, bx, j);
+                        else k_pml_box_aux<1, false><<<grd, blk, 0, stream>>>(a, bx, j);
+                    } else {
+                        if (psi) k_pml_box_aux<2, true><<<grd, blk, 0, stream>>>(a, bx, j);
+                        else k_pml_box_aux<2, false><<<grd, blk, 0, stream>>>(a, bx, j);
+                    }
+                    end();
+                    ++launches;
+                }
         }
     }
     if (a.src.n > 0 || a.rcv.n > 0) {
         begin(KK_SRC_RCV);
-        k_src_rcv<<<(unsigned)prm.batch, 128, 0, stream>>>(a, j, 1, 1);
+        if (inline_ok) k_src_rcv_inline<<<(unsigned)prm.batch, 256, 0, stream>>>(a, inl, j);
+        else k_src_rcv<<<(unsigned)prm.batch, 128, 0, stream>>>(a, j, 1, 1);
         end();
         ++launches;
     }
@@ -1149,7 +1453,9 @@ int64_t Engine::Impl::kernels_per_step() const {
     if (a.lrs.n > 0) ++k;
     if (a.pml.width > 0) {
         if (ref()) k += (nx > 4 && ny > 4 && nz > 4) ? 2 : 0;
-        else if (a.pml.n_cells > 0) k += 2;
+        else if (a.pml.n_units > 0)
+            k += (int64_t)pml_boxes.size() + (int64_t)pml_axis_boxes[0].size() + (int64_t)pml_axis_boxes[1].size() +
+                 (int64_t)pml_axis_boxes[2].size();
     }
     if (a.src.n > 0 || a.rcv.n > 0) ++k;
     return k;

@@ -242,16 +242,18 @@ def config_c1(variant="fixed", steps=2000, seed=1):
     return Config("c1-ref", (nx, ny, nz), vox, a, b, dx, c, dt, steps, [(src_cell, sig)], rcv, mode=0)
 
 
-def config_c2(steps=5000, seed=2):
+def config_c2(steps=5000, seed=2, dims=(512, 384, 320)):
     """512x384x320 (~63M cells), 4 materials with third-order filters
     (K = 4), 20 seeded furniture boxes, PML on two faces (x+ and z+),
-    band-limited white noise (50-2000 Hz, unit RMS), 32 receivers."""
-    nx, ny, nz = 512, 384, 320
+    band-limited white noise (50-2000 Hz, unit RMS), 32 receivers.
+    `dims` scales the same construction (profiling captures)."""
+    nx, ny, nz = dims
     dx, c = 0.025, 343.0
     dt = courant_dt(dx, c)
     fs = 1.0 / dt
     faces = FACE_XP | FACE_ZP
-    vox = room(nx, ny, nz, 63 & ~faces, n_boxes=20, nmat=4, seed=seed, box_min=8, box_max=60)
+    vox = room(nx, ny, nz, 63 & ~faces, n_boxes=20, nmat=4, seed=seed, box_min=8,
+               box_max=max(9, min(60, min(dims) // 3)))
     a, b = passive_filters(4, 4, seed + 100)
     src_cell = air_cells(vox, 1, seed + 200, margin=20)[0]
     rcv = air_cells(vox, 32, seed + 300, margin=3)

@@ -37,6 +37,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=None,
+                    help="NX,NY,NZ: the same construction at another size (profiling captures)")
+    ap.add_argument("--legs", default="device,e2e,roofline,cpu",
+                    help="comma list of device,e2e,roofline,cpu")
     return ap.parse_args()
 
 
@@ -148,12 +152,14 @@ def main():
     import __graft_entry__ as ge
     pkg = ge.load()
     W = pkg.workloads
-    cfg = W.config_c2(steps=max(args.steps, 1))
+    legs = set(args.legs.split(","))
+    dims = tuple(int(v) for v in args.grid.split(",")) if args.grid else (512, 384, 320)
+    cfg = W.config_c2(steps=max(args.steps, 1), dims=dims)
     nx, ny, nz = cfg.dims
     interior = (nx - 2) * (ny - 2) * (nz - 2)
     metric = "Mcell-updates/s"
-    config = {"workload": "512x384x320 single-source FP32 (4 materials K=4, 20 boxes, PML x+/z+ "
-                          "width 12, 32 receivers)", "grid": [nx, ny, nz], "interior_cells": interior,
+    config = {"workload": "%dx%dx%d single-source FP32 (4 materials K=4, 20 boxes, PML x+/z+ "
+                          "width 12, 32 receivers)" % (nx, ny, nz), "grid": [nx, ny, nz], "interior_cells": interior,
               "mode": "FIXED", "l2_flush": "not needed: three 252 MB field levels exceed the 126 MB L2",
               "parallelism": "replicas" if world > 1 else "single"}
 
@@ -191,6 +197,8 @@ def main():
 
     sim = make_sim()
     K, Wm = args.steps, max(args.warmup, 3)
+    if "device" not in legs:
+        legs.add("device")
     sim.Run(Wm)
     if world > 1:
         torch.distributed.barrier()
@@ -211,8 +219,26 @@ def main():
         ms = float(t.item())
     value = interior * K * world / (ms / 1e3) / 1e6
 
-    # end to end through the public API: per step the source sample goes
-    # host->device and the receiver samples come back device->host
+    line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": K, "warmup": Wm,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": config, "gpu_launches": launches, "clocks": clk}
+    if "e2e" in legs:
+        line["e2e"] = e2e_leg(sim, cfg, K, interior, world, metric)
+    sim.close()
+    if "roofline" in legs:
+        line["roofline"] = roofline_leg(make_sim, K, interior)
+    if rank == 0 and world == 1 and "cpu" in legs and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference(cfg, 4)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def e2e_leg(sim, cfg, K, interior, world, metric):
+    """Same metric through the public API: per step the source sample goes
+    host->device and the receiver samples come back device->host."""
+    import torch
     chunk = 200
     sig = np.ascontiguousarray(cfg.sources[0][1], dtype=np.float32)
     host_rcv = np.empty((len(cfg.receivers), chunk), np.float32)
@@ -234,11 +260,12 @@ def main():
         t = torch.tensor([e2e_ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e = {"value": interior * K * world / (e2e_ms / 1e3) / 1e6, "unit": metric,
-           "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * len(cfg.receivers)}
+    return {"value": interior * K * world / (e2e_ms / 1e3) / 1e6, "unit": metric,
+            "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * len(cfg.receivers)}
 
-    # roofline of the dominant kernel: per-launch CUDA events (profile mode)
-    sim.close()
+
+def roofline_leg(make_sim, K, interior):
+    """Roofline of the dominant kernel from per-launch CUDA events."""
     psim = make_sim(profile=1, graphs=0)
     psim.Run(min(K, 400) + 1)
     stats = psim.kernel_stats()
@@ -256,21 +283,10 @@ def main():
             traffic = json.load(open(tfile)).get(name)
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "bytes_per_launch": step_kernel_bytes, "avg_launch_ms": avg_ms,
-            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in stats.items()}}
-
-    line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": K, "warmup": Wm,
-            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "config": config, "e2e": e2e, "roofline": roof,
-            "gpu_launches": launches, "clocks": clk}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(cfg, 4)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+            "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in stats.items() if v[0]}}
 
 
 if __name__ == "__main__":
