@@ -32,7 +32,7 @@ EXPORTS = [
     "afd_default_params", "afd_version", "afd_device_name",
     "afd_model_load_kerkythea", "afd_model_from_voxels", "afd_model_dims", "afd_model_voxels",
     "afd_model_coefs", "afd_model_material_names", "afd_model_classify", "afd_model_group_points",
-    "afd_model_last_error", "afd_model_destroy", "afd_check_filters",
+    "afd_model_last_error", "afd_model_destroy", "afd_check_filters", "afd_check_filters_static",
     "afd_create", "afd_set_min_size", "afd_load", "afd_set_model", "afd_set_pml",
     "afd_set_pml_profile", "afd_add_source", "afd_add_source_cell", "afd_add_receiver",
     "afd_add_receiver_cell", "afd_run", "afd_get_receivers", "afd_update_source",
@@ -96,6 +96,7 @@ def library(path=LIB_PATH):
         "afd_model_last_error": (C.c_char_p, [vp]),
         "afd_model_destroy": (None, [vp]),
         "afd_check_filters": (C.c_int, [i32, i32, P(f64), P(f64), i32, P(i32), P(f64), P(f64)]),
+        "afd_check_filters_static": (C.c_int, [i32, i32, P(f64), P(f64), i32, P(i32), P(f64), P(f64)]),
         "afd_create": (C.c_int, [P(vp), P(Params)]),
         "afd_set_min_size": (C.c_int, [vp, f32, f32, f32]),
         "afd_load": (C.c_int, [vp, C.c_char_p]),

@@ -203,6 +203,14 @@ int afd_check_filters(int32_t nmat, int32_t ncoef, const double* a, const double
     });
 }
 
+int afd_check_filters_static(int32_t nmat, int32_t ncoef, const double* a, const double* b, int32_t n_freq,
+                             int32_t* status, double* min_real, double* max_root) {
+    if (nmat < 1 || ncoef < 1 || !a || !b || n_freq < 2 || !status) return AFD_ERR_ARG;
+    return guard(g_create_error, [&] {
+        afd::check_filters_static(nmat, ncoef, a, b, n_freq, status, min_real, max_root);
+    });
+}
+
 // ---- simulation -------------------------------------------------------------
 int afd_create(afd_sim** out, const afd_params* p) {
     if (!out) return AFD_ERR_ARG;

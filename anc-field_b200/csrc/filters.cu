@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -150,6 +151,88 @@ void check_filters(int32_t nmat, int32_t K, const double* a, const double* b, in
         status[m] = st;
         if (min_real) min_real[m] = lows[(size_t)m];
         if (max_root) max_root[m] = roots[(size_t)m];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the filter check.
+//
+// For callers that must not allocate device memory: a process that runs
+// under a fixed GPU memory budget set by its host application, or a
+// control thread that re-checks filter coefficients while a simulation is
+// running and may not grow or fragment the device heap. The scratch lives
+// in one file-scope device array; inputs and outputs stay host arrays.
+// Limits: nmat <= kStaticMaxMat materials, ncoef <= kStaticMaxCoef.
+// Every call reuses the same array, so calls that overlap on the GPU (from
+// several host threads, or on a device in use by another such call) race
+// and must be serialised by the caller. The first call on a device looks up
+// the array's device address (cudaGetSymbolAddress) with that device
+// current; make that first call before any stream capture.
+// ---------------------------------------------------------------------------
+constexpr int kStaticMaxMat = 64;
+constexpr int kStaticMaxCoef = 16;
+constexpr int kStaticBlocks = 8;
+constexpr int kStaticDoubles =
+    2 * kStaticMaxMat * kStaticMaxCoef + kStaticMaxMat + kStaticMaxMat * kStaticBlocks;
+static __device__ __align__(256) double g_filter_scratch[kStaticDoubles];
+
+static std::mutex g_scratch_mu;
+static double* g_scratch_ptr[256] = {};
+
+// Device address of g_filter_scratch on the current device (set up once).
+static double* scratch_on_current_device() {
+    int dev = 0;
+    CKF(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) throw Error(AFD_ERR_CUDA, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_filter_scratch);
+        if (e != cudaSuccess || !ptr)
+            throw Error(AFD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_scratch_ptr[dev] = static_cast<double*>(ptr);
+    }
+    return g_scratch_ptr[dev];
+}
+
+void check_filters_static(int32_t nmat, int32_t K, const double* a, const double* b, int32_t nf,
+                          int32_t* status, double* min_real, double* max_root) {
+    if (nmat > kStaticMaxMat || K > kStaticMaxCoef)
+        throw Error(AFD_ERR_ARG, "afd_check_filters_static: at most " + std::to_string(kStaticMaxMat) +
+                                     " materials of " + std::to_string(kStaticMaxCoef) +
+                                     " coefficients fit its fixed scratch (got " + std::to_string(nmat) + " x " +
+                                     std::to_string(K) + ")");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Error(AFD_ERR_CUDA, "afd_check_filters_static needs a CUDA device");
+    double* base = scratch_on_current_device();
+    double* da = base;
+    double* db = base + kStaticMaxMat * kStaticMaxCoef;
+    double* dr = base + 2 * kStaticMaxMat * kStaticMaxCoef;
+    double* dl = dr + kStaticMaxMat;
+    const size_t nab = (size_t)nmat * K;
+    CKF(cudaMemcpy(da, a, nab * sizeof(double), cudaMemcpyHostToDevice));
+    CKF(cudaMemcpy(db, b, nab * sizeof(double), cudaMemcpyHostToDevice));
+    // every result slot read below is written by this call's kernels; the
+    // slots are cleared anyway so that a failed launch cannot hand back the
+    // previous call's values
+    CKF(cudaMemset(dr, 0, (size_t)(kStaticMaxMat + kStaticMaxMat * kStaticBlocks) * sizeof(double)));
+    k_roots<<<(nmat + 63) / 64, 64>>>(db, nmat, K, dr);
+    k_passive<<<dim3(kStaticBlocks, nmat), 256>>>(da, db, nmat, K, nf, dl);
+    CKF(cudaGetLastError());
+    double roots[kStaticMaxMat];
+    double part[kStaticMaxMat * kStaticBlocks];
+    CKF(cudaMemcpy(roots, dr, (size_t)nmat * sizeof(double), cudaMemcpyDeviceToHost));
+    CKF(cudaMemcpy(part, dl, (size_t)nmat * kStaticBlocks * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int m = 0; m < nmat; ++m) {
+        double lo = INFINITY;
+        for (int k = 0; k < kStaticBlocks; ++k) lo = std::fmin(lo, part[m * kStaticBlocks + k]);
+        int st = 0;
+        if (!(roots[m] < 1.0)) st |= 1;
+        if (!(lo >= 0.0)) st |= 2;
+        status[m] = st;
+        if (min_real) min_real[m] = lo;
+        if (max_root) max_root[m] = roots[m];
     }
 }
 

@@ -15,6 +15,11 @@ namespace afd {
 void check_filters(int32_t nmat, int32_t ncoef, const double* a, const double* b, int32_t n_freq,
                    int32_t* status, double* min_real, double* max_root);
 
+// Same check with its device scratch in a fixed file-scope array instead
+// of cudaMalloc'd buffers (nmat <= 64, ncoef <= 16); needs a CUDA device.
+void check_filters_static(int32_t nmat, int32_t ncoef, const double* a, const double* b, int32_t n_freq,
+                          int32_t* status, double* min_real, double* max_root);
+
 // Name of CUDA device `index`; AFD_ERR_ARG past the end, AFD_ERR_CUDA
 // without a device.
 int device_name(int32_t index, std::string* name);

@@ -134,6 +134,20 @@ void afd_model_destroy(afd_model* m);
 int afd_check_filters(int32_t nmat, int32_t ncoef, const double* a, const double* b,
                       int32_t n_freq, int32_t* status, double* min_real, double* max_root);
 
+/* No counterpart in the reference. The same check as afd_check_filters for
+ * callers that must not allocate device memory (a process held to a fixed
+ * GPU memory budget by its host application, or a control thread that
+ * re-checks coefficients while simulations run and may not grow the device
+ * heap): its scratch is one file-scope device array of 64 materials x 16
+ * coefficients (about 21 KB, held by every device that loads the library
+ * until exit). Sizes beyond that return AFD_ERR_ARG. Needs a CUDA device.
+ * The first call on a device looks up the array's address with that device
+ * current; make it before any stream capture. All calls share the array:
+ * calls that overlap on the GPU race, so the caller serialises them. The
+ * error text is afd_model_last_error(NULL). */
+int afd_check_filters_static(int32_t nmat, int32_t ncoef, const double* a, const double* b,
+                             int32_t n_freq, int32_t* status, double* min_real, double* max_root);
+
 /* ------------------------------------------------------------------ */
 /* Simulation                                                          */
 /* ------------------------------------------------------------------ */
