@@ -105,6 +105,24 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value, device="cpu"):
+    """Maximum of a per-rank number over all ranks (the timing rule: a
+    multi-GPU time is the slowest rank's); the value itself with one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(cells_per_replica, steps, world, ms):
+    """Whole-job cell-updates/s in millions for `world` independent replicas
+    timed by the slowest one (weak scaling)."""
+    return cells_per_replica * steps * world / (ms / 1e3) / 1e6
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -213,11 +231,8 @@ def main():
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     launches = sim.info().kernel_launches
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = interior * K * world / (ms / 1e3) / 1e6
+    ms = max_over_ranks(ms, "cuda")
+    value = replica_rate(interior, K, world, ms)
 
     line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -255,12 +270,8 @@ def e2e_leg(sim, cfg, K, interior, world, metric):
         sim.mics_range(t0, t0 + n, out=host_rcv[:, :n] if n == chunk else None)
         done += n
     e2e_s = time.perf_counter() - w0
-    e2e_ms = e2e_s * 1e3
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    return {"value": interior * K * world / (e2e_ms / 1e3) / 1e6, "unit": metric,
+    e2e_ms = max_over_ranks(e2e_s * 1e3, "cuda")
+    return {"value": replica_rate(interior, K, world, e2e_ms), "unit": metric,
             "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * len(cfg.receivers)}
 
 
