@@ -6,6 +6,8 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace afd {
@@ -78,11 +80,26 @@ struct RcvDev {
     int64_t cap;
 };
 
+// FP16 field storage (AFD_STORE_FP16, FIXED scheme): the three levels as
+// binary16 holding p * s, one power-of-two scale s per stored level and
+// batch member. The scale of level L (written at global step L) follows
+// from the largest magnitude of level L - 2, which the interior kernel of
+// step L - 1 gathers while it reads that level as p^n (no extra pass):
+// mx[b * 5 + slot(L)] holds the float bits of max |level L| (atomicMax),
+// slot(L) = L mod 5. Step g gathers slot g - 1, reads slots g - 2 .. g - 4
+// and clears slot g for the next step.
+struct F16Dev {
+    __half* h[3];             // the three levels, each [batch][vol]
+    uint32_t* mx;             // [batch][5]
+    const float* src_max;     // [batch] largest |source sample| of the member
+};
+
 struct StepArgs {
     GridDev g;
     int32_t batch;
     int32_t mode;             // AFD_MODE_REF / AFD_MODE_FIXED
     float* p[3];              // three rotating field buffers, each [batch][vol]
+    F16Dev f16;
     const long long* d_step;  // global step index at the start of the chunk
     float lambda2, cint;      // interior: lambda^2 and 2(1-3 lambda^2)
     LrsDev lrs;
@@ -103,6 +120,93 @@ __host__ __device__ inline int buf_old(long long g) { return (buf_new(g) + 2) % 
 // before every step, starting from 0).
 __host__ __device__ inline int ring_index(long long g, int K) { return K - 1 - (int)(g % K); }
 
+// ---- FP16 storage ----------------------------------------------------------
+__host__ __device__ inline int max_slot(long long L) { return (int)(((L % 5) + 5) % 5); }
+
+// Scale of a level from the largest magnitude m of the level two steps
+// before it and the member's largest source sample smax: 2^(10 - e) with
+// m' = max(m, smax) < 2^e (frexp's exponent), 1 when m' is 0, exponent
+// clamped to [-60, 60]. The 2^6 headroom below the binary16 maximum covers
+// the growth of two steps.
+__host__ __device__ inline float level_scale(uint32_t mbits, float smax) {
+    float m;
+    memcpy(&m, &mbits, 4);
+    const float a = m > smax ? m : smax;
+    if (!(a > 0.0f)) return 1.0f;
+    uint32_t ab;
+    memcpy(&ab, &a, 4);
+    const int e = (int)((ab >> 23) & 0xffu) - 126;  // frexp exponent of a normal a
+    int k = 10 - e;
+    k = k > 60 ? 60 : (k < -60 ? -60 : k);
+    const uint32_t sb = (uint32_t)(k + 127) << 23;
+    float sc;
+    memcpy(&sc, &sb, 4);
+    return sc;
+}
+
+// Scales of the levels step g reads and writes for member b.
+struct StepScales {
+    float s_new, inv_new;  // level g
+    float s_cur, inv_cur;  // level g - 1 (p^n)
+    float s_old, inv_old;  // level g - 2 (p^{n-1})
+};
+
+__device__ __forceinline__ StepScales step_scales(const F16Dev& f, int b, long long g) {
+    const uint32_t* mx = f.mx + (size_t)b * 5;
+    const float smax = __ldg(f.src_max + b);
+    StepScales s;
+    s.s_new = level_scale(*(volatile const uint32_t*)(mx + max_slot(g - 2)), smax);
+    s.s_cur = level_scale(*(volatile const uint32_t*)(mx + max_slot(g - 3)), smax);
+    s.s_old = level_scale(*(volatile const uint32_t*)(mx + max_slot(g - 4)), smax);
+    s.inv_new = 1.0f / s.s_new;
+    s.inv_cur = 1.0f / s.s_cur;
+    s.inv_old = 1.0f / s.s_old;
+    return s;
+}
+
+// Loads and stores of a level as FP32 values: FP32 storage reads and
+// writes the value; FP16 storage decodes with 1/s and encodes v * s
+// (round to nearest even, exact scaling by a power of two).
+template <typename T>
+__device__ __forceinline__ float fld(const T* p, float inv) {
+    if constexpr (sizeof(T) == 4) {
+        (void)inv;
+        return *p;
+    } else {
+        return __half2float(*p) * inv;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ float fldg(const T* p, float inv) {
+    if constexpr (sizeof(T) == 4) {
+        (void)inv;
+        return __ldg(p);
+    } else {
+        return __half2float(__ldg(p)) * inv;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void fst(T* p, float v, float s) {
+    if constexpr (sizeof(T) == 4) {
+        (void)s;
+        *p = v;
+    } else {
+        *p = __float2half_rn(v * s);
+    }
+}
+
+// A stored FP16 value is finite when |v * s| < 65520 (binary16 overflow
+// threshold under round to nearest even).
+__device__ __forceinline__ bool f16_finite(float scaled) { return fabsf(scaled) < 65520.0f; }
+
+template <typename T>
+__device__ __forceinline__ T* level_ptr(const StepArgs& a, int buf) {
+    if constexpr (sizeof(T) == 4) return a.p[buf];
+    else return a.f16.h[buf];
+}
+
 // Interior SLF update, leapfrog.cl:41-53.
 __device__ __forceinline__ float slf_update(float lambda2, float cint, float xp, float xm, float yp,
                                             float ym, float zp, float zm, float c, float old) {
@@ -112,6 +216,24 @@ __device__ __forceinline__ float slf_update(float lambda2, float cint, float xp,
     s = s + zp;
     s = s + zm;
     return lambda2 * s + cint * c - old;
+}
+
+// The same update for FP16 storage, on stored values: c, the six
+// neighbours and old are p^n * s_cur and p^{n-1} * s_old; rc = s_new /
+// s_cur and ro = s_new / s_old are powers of two, so each operation equals
+// its unscaled counterpart times s_new exactly. Evaluated as
+// p + ((p - p^{n-1}) + lambda^2 (S - 6p)): the increment is formed before
+// it is added to the level.
+__device__ __forceinline__ float slf_update_scaled(float lambda2, float rc, float ro, float xp, float xm,
+                                                   float yp, float ym, float zp, float zm, float c,
+                                                   float old) {
+    float s = xp + xm;
+    s = s + yp;
+    s = s + ym;
+    s = s + zp;
+    s = s + zm;
+    const float S = s * rc, p = c * rc, o = old * ro;
+    return p + ((p - o) + lambda2 * (S - 6.0f * p));
 }
 
 // Neighbour sum of a boundary cell: axes in x, y, z order; a wall on the +

@@ -65,7 +65,10 @@ __device__ __forceinline__ void watch(int* flag, float v) {
     if (!(fabsf(v) < 1e30f)) atomicOr(flag, 1);
 }
 
-// leapfrog.cl:34-55 over 1 <= x,y,z <= n-2 of every batch member.
+// leapfrog.cl:34-55 over 1 <= x,y,z <= n-2 of every batch member. FP16
+// storage: the update on stored values and the largest |p^n| gathered per
+// warp, as in k_stream.
+template <typename T>
 __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
     const long long g = *a.d_step + j;
     const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -73,55 +76,92 @@ __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
     const int zn = a.g.nz - 2;
     const int b = blockIdx.z / zn;
     const int z = 1 + blockIdx.z % zn;
-    if (x > a.g.nx - 2 || y > a.g.ny - 2) return;
     const size_t base = (size_t)b * a.g.vol;
-    float* pn = a.p[buf_new(g)] + base;
-    const float* pc = a.p[buf_cur(g)] + base;
-    const float* po = a.p[buf_old(g)] + base;
     const int64_t i = (int64_t)z * a.g.plane + (int64_t)y * a.g.pitch + x;
-    const float v = slf_update(a.lambda2, a.cint, pc[i + 1], pc[i - 1], pc[i + a.g.pitch],
-                               pc[i - a.g.pitch], pc[i + a.g.plane], pc[i - a.g.plane], pc[i], po[i]);
-    pn[i] = v;
-    watch(a.flag, v);
+    if constexpr (sizeof(T) == 4) {
+        if (x > a.g.nx - 2 || y > a.g.ny - 2) return;
+        float* pn = a.p[buf_new(g)] + base;
+        const float* pc = a.p[buf_cur(g)] + base;
+        const float* po = a.p[buf_old(g)] + base;
+        const float v = slf_update(a.lambda2, a.cint, pc[i + 1], pc[i - 1], pc[i + a.g.pitch],
+                                   pc[i - a.g.pitch], pc[i + a.g.plane], pc[i - a.g.plane], pc[i], po[i]);
+        pn[i] = v;
+        watch(a.flag, v);
+    } else {
+        if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+            for (int m = 0; m < a.batch; ++m) a.f16.mx[(size_t)m * 5 + max_slot(g)] = 0u;
+        const bool in = x <= a.g.nx - 2 && y <= a.g.ny - 2;
+        const StepScales sc = step_scales(a.f16, b, g);
+        uint32_t amax = 0;
+        if (in) {
+            __half* pn = a.f16.h[buf_new(g)] + base;
+            const __half* pc = a.f16.h[buf_cur(g)] + base;
+            const __half* po = a.f16.h[buf_old(g)] + base;
+            const float v = slf_update_scaled(
+                a.lambda2, sc.s_new * sc.inv_cur, sc.s_new * sc.inv_old, __half2float(pc[i + 1]),
+                __half2float(pc[i - 1]), __half2float(pc[i + a.g.pitch]), __half2float(pc[i - a.g.pitch]),
+                __half2float(pc[i + a.g.plane]), __half2float(pc[i - a.g.plane]), __half2float(pc[i]),
+                __half2float(po[i]));
+            pn[i] = __float2half_rn(v);
+            if (!f16_finite(v)) atomicOr(a.flag, 1);
+            amax = __half_as_ushort(pc[i]) & 0x7fffu;
+        }
+        const uint32_t wmax = __reduce_max_sync(0xffffffffu, amax);
+        if ((threadIdx.x & 31) == 0 && wmax)
+            atomicMax(a.f16.mx + (size_t)b * 5 + max_slot(g - 1),
+                      __float_as_uint(__half2float(__ushort_as_half((unsigned short)wmax)) * sc.inv_cur));
+    }
 }
 
 // The 26 lrs_k launches of simulation.hpp:366-370 as one launch over the
 // compact list.
 // KT: filter length fixed at compile time (1..4), 0 for any length.
-template <bool REF, int KT>
+// T: level storage (FP16 only with the FIXED scheme).
+template <bool REF, int KT, typename T>
 __global__ void __launch_bounds__(256) k_lrs(const __grid_constant__ StepArgs a, int j) {
     const long long g = *a.d_step + j;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.lrs.n) return;
     const int b = blockIdx.y;
     const size_t base = (size_t)b * a.g.vol;
-    float* pn = a.p[buf_new(g)] + base;
-    const float* pc = a.p[buf_cur(g)] + base;
-    const float* po = a.p[buf_old(g)] + base;
+    T* pn = level_ptr<T>(a, buf_new(g)) + base;
+    const T* pc = level_ptr<T>(a, buf_cur(g)) + base;
+    const T* po = level_ptr<T>(a, buf_old(g)) + base;
+    float s_new = 1.0f, ic = 1.0f, io = 1.0f;
+    if constexpr (sizeof(T) == 2) {
+        const StepScales sc = step_scales(a.f16, b, g);
+        s_new = sc.s_new;
+        ic = sc.inv_cur;
+        io = sc.inv_old;
+    }
     const int64_t c = __ldg(a.lrs.cell + e);
     const uint32_t info = __ldg(a.lrs.info + e);
-    const float nb[6] = {__ldg(pc + c + 1), __ldg(pc + c - 1), __ldg(pc + c + a.g.pitch),
-                         __ldg(pc + c - a.g.pitch), __ldg(pc + c + a.g.plane), __ldg(pc + c - a.g.plane)};
+    const float nb[6] = {fldg(pc + c + 1, ic), fldg(pc + c - 1, ic), fldg(pc + c + a.g.pitch, ic),
+                         fldg(pc + c - a.g.pitch, ic), fldg(pc + c + a.g.plane, ic), fldg(pc + c - a.g.plane, ic)};
     const int grp = (int)(info & 31u);
     const int ix_buf = ring_index(g, a.lrs.K);
     float v;
     if (grp < 6) {
-        v = lrs_face<KT>(a.lrs, e, b, grp, (int)((info >> 5) & 255u), nb, __ldg(pc + c), __ldg(po + c), ix_buf);
+        v = lrs_face<KT>(a.lrs, e, b, grp, (int)((info >> 5) & 255u), nb, fldg(pc + c, ic), fldg(po + c, io),
+                         ix_buf);
     } else {
-        const float pint = (REF && grp == 25) ? pn[c] : 0.0f;
-        v = lrs_point<REF, KT>(a.lrs, e, b, info, nb, __ldg(pc + c), __ldg(po + c), pint, ix_buf);
+        const float pint = (REF && grp == 25) ? fld(pn + c, 1.0f) : 0.0f;
+        v = lrs_point<REF, KT>(a.lrs, e, b, info, nb, fldg(pc + c, ic), fldg(po + c, io), pint, ix_buf);
     }
-    pn[c] = v;
+    fst(pn + c, v, s_new);
+    if constexpr (sizeof(T) == 2) {
+        if (!f16_finite(v * s_new)) atomicOr(a.flag, 1);
+    }
 }
 
-template <bool REF>
+template <bool REF, typename T>
 static void launch_lrs(const StepArgs& a, int j, dim3 grd, cudaStream_t st) {
     switch (a.lrs.K) {
-        case 1: k_lrs<REF, 1><<<grd, 256, 0, st>>>(a, j); break;
-        case 2: k_lrs<REF, 2><<<grd, 256, 0, st>>>(a, j); break;
-        case 3: k_lrs<REF, 3><<<grd, 256, 0, st>>>(a, j); break;
-        case 4: k_lrs<REF, 4><<<grd, 256, 0, st>>>(a, j); break;
-        default: k_lrs<REF, 0><<<grd, 256, 0, st>>>(a, j); break;
+        case 1: k_lrs<REF, 1, T><<<grd, 256, 0, st>>>(a, j); break;
+        case 2: k_lrs<REF, 2, T><<<grd, 256, 0, st>>>(a, j); break;
+        case 3: k_lrs<REF, 3, T><<<grd, 256, 0, st>>>(a, j); break;
+        case 4: k_lrs<REF, 4, T><<<grd, 256, 0, st>>>(a, j); break;
+        default: k_lrs<REF, 0, T><<<grd, 256, 0, st>>>(a, j); break;
     }
 }
 
@@ -349,11 +389,48 @@ __device__ __forceinline__ void store4(float* p, const float v[4], unsigned m) {
     }
 }
 
+// The same for a pressure level of either storage: FP16 rows decode with
+// 1/s (eight-byte loads of four values) and stores encode v * s.
+template <typename T>
+__device__ __forceinline__ void row5t(const T* p, float r[5], float inv) {
+    if constexpr (sizeof(T) == 4) {
+        (void)inv;
+        row5(p, r);
+    } else {
+        const uint2 w = __ldg(reinterpret_cast<const uint2*>(p));
+        const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+        const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+        r[0] = lo.x * inv;
+        r[1] = lo.y * inv;
+        r[2] = hi.x * inv;
+        r[3] = hi.y * inv;
+        r[4] = __half2float(__ldg(p + 4)) * inv;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void store4t(T* p, const float v[4], unsigned m, float s) {
+    if constexpr (sizeof(T) == 4) {
+        (void)s;
+        store4(p, v, m);
+    } else if (m == 15u) {
+        const __half2 lo = __floats2half2_rn(v[0] * s, v[1] * s), hi = __floats2half2_rn(v[2] * s, v[3] * s);
+        uint2 w;
+        w.x = *reinterpret_cast<const uint32_t*>(&lo);
+        w.y = *reinterpret_cast<const uint32_t*>(&hi);
+        *reinterpret_cast<uint2*>(p) = w;
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (m & (1u << q)) p[q] = __float2half_rn(v[q] * s);
+    }
+}
+
 // Pressure of the PML cells (pml.cl:185-207 restricted to the slab cells)
 // over one box of the disjoint box cover, four consecutive cells per
 // thread. Fields outside the read axes are identically zero there and are
 // not loaded; PSI: psi is kept (PML faces on all three axes).
-template <bool PSI>
+template <bool PSI, typename T>
 __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepArgs a, const PmlBox bx, int j) {
     int b, x, y, z;
     if (!box_cell(bx, b, x, y, z)) return;
@@ -364,18 +441,25 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
     const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
-    const float* pc = a.p[buf_cur(g)] + base;
-    const float* po = a.p[buf_old(g)] + base;
-    float* pn = a.p[buf_new(g)] + base;
+    const T* pc = level_ptr<T>(a, buf_cur(g)) + base;
+    const T* po = level_ptr<T>(a, buf_old(g)) + base;
+    T* pn = level_ptr<T>(a, buf_new(g)) + base;
+    float s_new = 1.0f, ic = 1.0f, io = 1.0f;
+    if constexpr (sizeof(T) == 2) {
+        const StepScales sc = step_scales(a.f16, b, g);
+        s_new = sc.s_new;
+        ic = sc.inv_cur;
+        io = sc.inv_old;
+    }
     const int lv = pml_level(a, g);
     float c[5], ym4[5], yp4[5], zm4[5], zp4[5], o[5];
-    row5(pc + i, c);
-    const float xm = __ldg(pc + i - 1);
-    row5(pc + i - pitch, ym4);
-    row5(pc + i + pitch, yp4);
-    row5(pc + i - plane, zm4);
-    row5(pc + i + plane, zp4);
-    row5(po + i, o);
+    row5t(pc + i, c, ic);
+    const float xm = fldg(pc + i - 1, ic);
+    row5t(pc + i - pitch, ym4, ic);
+    row5t(pc + i + pitch, yp4, ic);
+    row5t(pc + i - plane, zm4, ic);
+    row5t(pc + i + plane, zp4, ic);
+    row5t(po + i, o, io);
     const float4 kx4 = __ldg(reinterpret_cast<const float4*>(P.ksi[0] + x));
     const float kxv[4] = {kx4.x, kx4.y, kx4.z, kx4.w};
     const float ky = __ldg(P.ksi[1] + y), kz = __ldg(P.ksi[2] + z);
@@ -453,16 +537,20 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
         const float F = ks * o[q];
         const float num = A + B - C - D - E + F;
         v[q] = num / (P.inv_dt2 + ks);
-        if ((m >> q) & 1u) watch(a.flag, v[q]);
+        if constexpr (sizeof(T) == 4) {
+            if ((m >> q) & 1u) watch(a.flag, v[q]);
+        } else {
+            if (((m >> q) & 1u) && !f16_finite(v[q] * s_new)) atomicOr(a.flag, 1);
+        }
     }
-    store4(pn + i, v, m);
+    store4t(pn + i, v, m, s_new);
 }
 
 // Auxiliary field AX of the PML cells of one slab box (pml.cl:231-262 with
 // the derivative and ksi index corrected). The derivatives of the new and
 // previous pressure along every axis come from the same four rows
 // (y, y+1) x (z, z+1), x..x+4.
-template <int AX, bool PSI>
+template <int AX, bool PSI, typename T>
 __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ StepArgs a, const PmlBox bx,
                                                      int j) {
     int b, x, y, z;
@@ -474,18 +562,24 @@ __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ Ste
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
     const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
-    const float* pn = a.p[buf_new(g)] + base + i;
-    const float* pc = a.p[buf_cur(g)] + base + i;
+    const T* pn = level_ptr<T>(a, buf_new(g)) + base + i;
+    const T* pc = level_ptr<T>(a, buf_cur(g)) + base + i;
+    float in_ = 1.0f, ic = 1.0f;
+    if constexpr (sizeof(T) == 2) {
+        const StepScales sc = step_scales(a.f16, b, g);
+        in_ = sc.inv_new;
+        ic = sc.inv_cur;
+    }
     const int lv = pml_level(a, g);
     float n00[5], n01[5], n10[5], n11[5], m00[5], m01[5], m10[5], m11[5];
-    row5(pn, n00);
-    row5(pn + plane, n01);
-    row5(pn + pitch, n10);
-    row5(pn + pitch + plane, n11);
-    row5(pc, m00);
-    row5(pc + plane, m01);
-    row5(pc + pitch, m10);
-    row5(pc + pitch + plane, m11);
+    row5t(pn, n00, in_);
+    row5t(pn + plane, n01, in_);
+    row5t(pn + pitch, n10, in_);
+    row5t(pn + pitch + plane, n11, in_);
+    row5t(pc, m00, ic);
+    row5t(pc + plane, m01, ic);
+    row5t(pc + pitch, m10, ic);
+    row5t(pc + pitch + plane, m11, ic);
     float s00[5] = {0}, s01[5] = {0}, s10[5] = {0}, s11[5] = {0};
     if (PSI) {
         const float* ps = P.psi[lv] + base + i;
@@ -555,13 +649,17 @@ __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ Ste
 // Interior SLF update of every cell 1..n-2 (leapfrog.cl:34-55) streamed
 // through shared memory; see fused.cuh. Consumer warps wait on the stage
 // barriers independently (no block-wide barrier), so a slow warp delays
-// only its own rows.
+// only its own rows. T = __half: FP16 levels, the update evaluated on the
+// stored values (slf_update_scaled) and the largest |p^n| of every work
+// item gathered for the scale of level g + 1.
+template <typename T>
 __global__ void __launch_bounds__(F_THREADS, 2)
     k_stream(const __grid_constant__ CUtensorMap tm_halo, const __grid_constant__ CUtensorMap tm_own,
              const __grid_constant__ StepArgs a, const __grid_constant__ FusedDev f, int j) {
+    using TL = Tile<T>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + F_STAGES * F_STAGE_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + F_STAGES * TL::STAGE);
     uint64_t* empty = full + F_STAGES;
     int* slot = reinterpret_cast<int*>(empty + F_STAGES);  // work item of the stage that starts it
     const int tid = threadIdx.x;
@@ -582,6 +680,11 @@ __global__ void __launch_bounds__(F_THREADS, 2)
         // producer: takes work items from the launch's counter and streams
         // their planes; a stage with item -1 tells the consumers to stop
         if (tid == F_CONSUMERS) {
+            if constexpr (sizeof(T) == 2) {
+                // level g's maximum is gathered by the next step
+                if (blockIdx.x == 0)
+                    for (int b = 0; b < B; ++b) a.f16.mx[(size_t)b * 5 + max_slot(g)] = 0u;
+            }
             uint32_t k = 0;
             bool ok = true;
             while (ok) {
@@ -609,10 +712,10 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                         atomicOr(a.flag, 2);
                         break;
                     }
-                    unsigned char* st = smem + s * F_STAGE_BYTES;
-                    mbar_expect_tx(&full[s], F_TX_BYTES);
-                    tma_load_3d(st, &tm_halo, x0 - 4, y0 - 1, zc + z, &full[s]);
-                    tma_load_3d(st + F_PN_PAD, &tm_own, x0, y0, zo + z, &full[s]);
+                    unsigned char* st = smem + s * TL::STAGE;
+                    mbar_expect_tx(&full[s], TL::TX);
+                    tma_load_3d(st, &tm_halo, x0 - TL::XOFF, y0 - 1, zc + z, &full[s]);
+                    tma_load_3d(st + TL::PN_PAD, &tm_own, x0, y0, zo + z, &full[s]);
                 }
             }
             // wait for the last copy issued into every stage before leaving
@@ -637,7 +740,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
         if (item < 0) break;
         const FusedItem it = fused_item(f, item, nz);
         const int x = it.tx * FT_X + cx, y = it.ty * FT_Y + cy;
-        float* pn = a.p[wn] + (size_t)it.b * a.g.vol + (int64_t)y * a.g.pitch + x;
+        T* pn = level_ptr<T>(a, wn) + (size_t)it.b * a.g.vol + (int64_t)y * a.g.pitch + x;
         const bool yok = (y >= 1 && y <= a.g.ny - 2);
         const bool xfull = (x >= 1 && x + 3 <= a.g.nx - 2);
         const int planes = it.z1 - it.z0;
@@ -646,43 +749,111 @@ __global__ void __launch_bounds__(F_THREADS, 2)
             return;
         }
         bool bad = false;
-        for (int pl = 0; pl < planes; ++pl) {
-            const int z = it.z0 + pl;
-            const uint32_t kc = k + 1 + pl, kp = kc + 1, km = kc - 1;
-            if (!mbar_wait(&full[kp % F_STAGES], (kp / F_STAGES) & 1)) {
-                if (lane == 0) atomicOr(a.flag, 2);
-                return;
-            }
-            const float* P0 = reinterpret_cast<const float*>(smem + (kc % F_STAGES) * F_STAGE_BYTES);
-            const float* Pm = reinterpret_cast<const float*>(smem + (km % F_STAGES) * F_STAGE_BYTES);
-            const float* Pp = reinterpret_cast<const float*>(smem + (kp % F_STAGES) * F_STAGE_BYTES);
-            const float* O = reinterpret_cast<const float*>(smem + (kc % F_STAGES) * F_STAGE_BYTES + F_PN_PAD);
-            const int s0 = (cy + 1) * FH_X + cx + 4;
-            const float4 c = *reinterpret_cast<const float4*>(P0 + s0);
-            const float xm = P0[s0 - 1], xp = P0[s0 + 4];
-            const float4 ym = *reinterpret_cast<const float4*>(P0 + s0 - FH_X);
-            const float4 yp = *reinterpret_cast<const float4*>(P0 + s0 + FH_X);
-            const float4 zm = *reinterpret_cast<const float4*>(Pm + s0);
-            const float4 zp = *reinterpret_cast<const float4*>(Pp + s0);
-            const float4 o = *reinterpret_cast<const float4*>(O + cy * FT_X + cx);
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
-            float4 v;
-            v.x = slf_update(L2, CI, c.y, xm, yp.x, ym.x, zp.x, zm.x, c.x, o.x);
-            v.y = slf_update(L2, CI, c.z, c.x, yp.y, ym.y, zp.y, zm.y, c.y, o.y);
-            v.z = slf_update(L2, CI, c.w, c.y, yp.z, ym.z, zp.z, zm.z, c.z, o.z);
-            v.w = slf_update(L2, CI, xp, c.z, yp.w, ym.w, zp.w, zm.w, c.w, o.w);
-            bad |= !(fabsf(v.x) < 1e30f && fabsf(v.y) < 1e30f && fabsf(v.z) < 1e30f && fabsf(v.w) < 1e30f);
-            if (yok) {
-                float* dst = pn + (int64_t)z * a.g.plane;
-                if (xfull) {
-                    __stcs(reinterpret_cast<float4*>(dst), v);
-                } else {
-                    const float vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        if (x + m >= 1 && x + m <= a.g.nx - 2) dst[m] = vv[m];
+        if constexpr (sizeof(T) == 4) {
+            for (int pl = 0; pl < planes; ++pl) {
+                const int z = it.z0 + pl;
+                const uint32_t kc = k + 1 + pl, kp = kc + 1, km = kc - 1;
+                if (!mbar_wait(&full[kp % F_STAGES], (kp / F_STAGES) & 1)) {
+                    if (lane == 0) atomicOr(a.flag, 2);
+                    return;
                 }
+                const float* P0 = reinterpret_cast<const float*>(smem + (kc % F_STAGES) * TL::STAGE);
+                const float* Pm = reinterpret_cast<const float*>(smem + (km % F_STAGES) * TL::STAGE);
+                const float* Pp = reinterpret_cast<const float*>(smem + (kp % F_STAGES) * TL::STAGE);
+                const float* O = reinterpret_cast<const float*>(smem + (kc % F_STAGES) * TL::STAGE + TL::PN_PAD);
+                const int s0 = (cy + 1) * TL::HX + cx + TL::XOFF;
+                const float4 c = *reinterpret_cast<const float4*>(P0 + s0);
+                const float xm = P0[s0 - 1], xp = P0[s0 + 4];
+                const float4 ym = *reinterpret_cast<const float4*>(P0 + s0 - TL::HX);
+                const float4 yp = *reinterpret_cast<const float4*>(P0 + s0 + TL::HX);
+                const float4 zm = *reinterpret_cast<const float4*>(Pm + s0);
+                const float4 zp = *reinterpret_cast<const float4*>(Pp + s0);
+                const float4 o = *reinterpret_cast<const float4*>(O + cy * FT_X + cx);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
+                float4 v;
+                v.x = slf_update(L2, CI, c.y, xm, yp.x, ym.x, zp.x, zm.x, c.x, o.x);
+                v.y = slf_update(L2, CI, c.z, c.x, yp.y, ym.y, zp.y, zm.y, c.y, o.y);
+                v.z = slf_update(L2, CI, c.w, c.y, yp.z, ym.z, zp.z, zm.z, c.z, o.z);
+                v.w = slf_update(L2, CI, xp, c.z, yp.w, ym.w, zp.w, zm.w, c.w, o.w);
+                bad |= !(fabsf(v.x) < 1e30f && fabsf(v.y) < 1e30f && fabsf(v.z) < 1e30f && fabsf(v.w) < 1e30f);
+                if (yok) {
+                    float* dst = pn + (int64_t)z * a.g.plane;
+                    if (xfull) {
+                        __stcs(reinterpret_cast<float4*>(dst), v);
+                    } else {
+                        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            if (x + m >= 1 && x + m <= a.g.nx - 2) dst[m] = vv[m];
+                    }
+                }
+            }
+        } else {
+            const StepScales sc = step_scales(a.f16, it.b, g);
+            const float rc = sc.s_new * sc.inv_cur, ro = sc.s_new * sc.inv_old;
+            // cells of this thread's row that are grid-interior: their |p^n|
+            // (binary16 magnitude bits order as the values) enter the maximum
+            const uint32_t mlo = (yok && x >= 1 && x <= a.g.nx - 2 ? 0x7fffu : 0u) |
+                                 (yok && x + 1 >= 1 && x + 1 <= a.g.nx - 2 ? 0x7fff0000u : 0u);
+            const uint32_t mhi = (yok && x + 2 >= 1 && x + 2 <= a.g.nx - 2 ? 0x7fffu : 0u) |
+                                 (yok && x + 3 >= 1 && x + 3 <= a.g.nx - 2 ? 0x7fff0000u : 0u);
+            uint32_t amax = 0;
+            for (int pl = 0; pl < planes; ++pl) {
+                const int z = it.z0 + pl;
+                const uint32_t kc = k + 1 + pl, kp = kc + 1, km = kc - 1;
+                if (!mbar_wait(&full[kp % F_STAGES], (kp / F_STAGES) & 1)) {
+                    if (lane == 0) atomicOr(a.flag, 2);
+                    return;
+                }
+                const __half* P0 = reinterpret_cast<const __half*>(smem + (kc % F_STAGES) * TL::STAGE);
+                const __half* Pm = reinterpret_cast<const __half*>(smem + (km % F_STAGES) * TL::STAGE);
+                const __half* Pp = reinterpret_cast<const __half*>(smem + (kp % F_STAGES) * TL::STAGE);
+                const __half* O =
+                    reinterpret_cast<const __half*>(smem + (kc % F_STAGES) * TL::STAGE + TL::PN_PAD);
+                const int s0 = (cy + 1) * TL::HX + cx + TL::XOFF;
+                const uint2 cr = *reinterpret_cast<const uint2*>(P0 + s0);
+                const float xm = __half2float(P0[s0 - 1]), xp = __half2float(P0[s0 + 4]);
+                const uint2 ymr = *reinterpret_cast<const uint2*>(P0 + s0 - TL::HX);
+                const uint2 ypr = *reinterpret_cast<const uint2*>(P0 + s0 + TL::HX);
+                const uint2 zmr = *reinterpret_cast<const uint2*>(Pm + s0);
+                const uint2 zpr = *reinterpret_cast<const uint2*>(Pp + s0);
+                const uint2 orw = *reinterpret_cast<const uint2*>(O + cy * FT_X + cx);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
+                amax = max(amax, max(max(cr.x & mlo & 0x7fffu, (cr.x & mlo) >> 16),
+                                     max(cr.y & mhi & 0x7fffu, (cr.y & mhi) >> 16)));
+                auto h2 = [](uint32_t w) { return __half22float2(*reinterpret_cast<const __half2*>(&w)); };
+                const float2 c01 = h2(cr.x), c23 = h2(cr.y);
+                const float2 ym01 = h2(ymr.x), ym23 = h2(ymr.y), yp01 = h2(ypr.x), yp23 = h2(ypr.y);
+                const float2 zm01 = h2(zmr.x), zm23 = h2(zmr.y), zp01 = h2(zpr.x), zp23 = h2(zpr.y);
+                const float2 o01 = h2(orw.x), o23 = h2(orw.y);
+                float4 v;
+                v.x = slf_update_scaled(L2, rc, ro, c01.y, xm, yp01.x, ym01.x, zp01.x, zm01.x, c01.x, o01.x);
+                v.y = slf_update_scaled(L2, rc, ro, c23.x, c01.x, yp01.y, ym01.y, zp01.y, zm01.y, c01.y, o01.y);
+                v.z = slf_update_scaled(L2, rc, ro, c23.y, c01.y, yp23.x, ym23.x, zp23.x, zm23.x, c23.x, o23.x);
+                v.w = slf_update_scaled(L2, rc, ro, xp, c23.x, yp23.y, ym23.y, zp23.y, zm23.y, c23.y, o23.y);
+                bad |= !(f16_finite(v.x) && f16_finite(v.y) && f16_finite(v.z) && f16_finite(v.w));
+                if (yok) {
+                    __half* dst = pn + (int64_t)z * a.g.plane;
+                    if (xfull) {
+                        const __half2 lo = __floats2half2_rn(v.x, v.y), hi = __floats2half2_rn(v.z, v.w);
+                        uint2 w;
+                        w.x = *reinterpret_cast<const uint32_t*>(&lo);
+                        w.y = *reinterpret_cast<const uint32_t*>(&hi);
+                        __stcs(reinterpret_cast<uint2*>(dst), w);
+                    } else {
+                        const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            if (x + m >= 1 && x + m <= a.g.nx - 2) dst[m] = __float2half_rn(vv[m]);
+                    }
+                }
+            }
+            const uint32_t wmax = __reduce_max_sync(0xffffffffu, amax);
+            if (lane == 0 && wmax) {
+                const float m = __half2float(__ushort_as_half((unsigned short)wmax)) * sc.inv_cur;
+                atomicMax(a.f16.mx + (size_t)it.b * 5 + max_slot(g - 1), __float_as_uint(m));
             }
         }
         __syncwarp();
@@ -695,24 +866,40 @@ __global__ void __launch_bounds__(F_THREADS, 2)
     }
 }
 
+// Scale and inverse scale of level g for member b (1 for FP32 storage).
+template <typename T>
+__device__ __forceinline__ float2 new_level_scale(const StepArgs& a, int b, long long g) {
+    if constexpr (sizeof(T) == 4) {
+        return make_float2(1.0f, 1.0f);
+    } else {
+        const float s = level_scale(*(volatile const uint32_t*)(a.f16.mx + (size_t)b * 5 + max_slot(g - 2)),
+                                    __ldg(a.f16.src_max + b));
+        return make_float2(s, 1.0f / s);
+    }
+}
+
 // source.cl:32-40 then mic.cl:32-41 for one batch member per block.
 // Sources landing on one cell are added in insertion order.
+template <typename T>
 __global__ void k_src_rcv(StepArgs a, int j, int do_src, int do_rcv) {
     const long long g = *a.d_step + j;
     const int b = blockIdx.x;
-    float* pn = a.p[buf_new(g)] + (size_t)b * a.g.vol;
+    T* pn = level_ptr<T>(a, buf_new(g)) + (size_t)b * a.g.vol;
+    const float2 sc = new_level_scale<T>(a, b, g);
     if (do_src && threadIdx.x == 0) {
         for (int s = a.src.begin[b]; s < a.src.begin[b + 1]; ++s) {
             const float v = (g < a.src.len[s]) ? a.src.data[a.src.off[s] + g] : 0.0f;
-            pn[a.src.cell[s]] += v;
+            T* c = pn + a.src.cell[s];
+            fst(c, fld(c, sc.y) + v, sc.x);
         }
     }
     __syncthreads();
     if (!do_rcv) return;
     for (int r = threadIdx.x; r < a.rcv.n; r += blockDim.x) {
-        const float v = pn[a.rcv.cell[r]];
+        const float v = fld(pn + a.rcv.cell[r], sc.y);
         a.rcv.out[((size_t)b * a.rcv.n + r) * a.rcv.cap + g] = v;
-        watch(a.flag, v);
+        if constexpr (sizeof(T) == 4) watch(a.flag, v);
+        else if (!f16_finite(v * sc.x)) atomicOr(a.flag, 1);
     }
 }
 
@@ -728,23 +915,27 @@ struct SrcRcvInline {
     int32_t rcv_cell[kInlineRcv];
 };
 
+template <typename T>
 __global__ void k_src_rcv_inline(const __grid_constant__ StepArgs a, const __grid_constant__ SrcRcvInline q,
                                  int j) {
     const long long g = *a.d_step + j;
     const int b = blockIdx.x;
-    float* pn = a.p[buf_new(g)] + (size_t)b * a.g.vol;
+    T* pn = level_ptr<T>(a, buf_new(g)) + (size_t)b * a.g.vol;
+    const float2 sc = new_level_scale<T>(a, b, g);
     if (threadIdx.x == 0) {
         for (int s = 0; s < q.n_src; ++s) {
             if (q.src_batch[s] != b) continue;
             const float v = (g < q.src_len[s]) ? __ldg(q.src_ptr[s] + g) : 0.0f;
-            pn[q.src_cell[s]] += v;
+            T* c = pn + q.src_cell[s];
+            fst(c, fld(c, sc.y) + v, sc.x);
         }
     }
     __syncthreads();
     for (int r = threadIdx.x; r < q.n_rcv; r += blockDim.x) {
-        const float v = pn[q.rcv_cell[r]];
+        const float v = fld(pn + q.rcv_cell[r], sc.y);
         a.rcv.out[((size_t)b * q.n_rcv + r) * a.rcv.cap + g] = v;
-        watch(a.flag, v);
+        if constexpr (sizeof(T) == 4) watch(a.flag, v);
+        else if (!f16_finite(v * sc.x)) atomicOr(a.flag, 1);
     }
 }
 
@@ -754,30 +945,40 @@ __global__ void k_advance(long long* d_step, int n) { *d_step += n; }
 // in FP64: 1/2 sum (u1-u0)^2 + lambda2/2 sum over grid edges of
 // (u1_i-u1_j)(u0_i-u0_j), over the cells 1..n-2 and their edges (edges to
 // the fixed outer faces included once).
-__global__ void k_energy(const float* u1, const float* u0, GridDev g, double lambda2, double* out) {
+template <typename T>
+__global__ void k_energy(const T* u1_, const T* u0_, float inv1, float inv0, GridDev g, double lambda2,
+                         double* out) {
+    auto u1 = [&](int64_t k) { return (double)fld(u1_ + k, inv1); };
+    auto u0 = [&](int64_t k) { return (double)fld(u0_ + k, inv0); };
     const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int z = 1 + blockIdx.z;
     double acc = 0.0;
     if (x <= g.nx - 2 && y <= g.ny - 2) {
         const int64_t i = (int64_t)z * g.plane + (int64_t)y * g.pitch + x;
-        const double d = (double)u1[i] - (double)u0[i];
+        const double d = u1(i) - u0(i);
         acc = 0.5 * d * d;
         const int64_t off[3] = {1, g.pitch, g.plane};
         const int lo[3] = {x, y, z};
         double pot = 0.0;
         for (int ax = 0; ax < 3; ++ax) {
             const int64_t jp = i + off[ax];
-            pot += ((double)u1[i] - (double)u1[jp]) * ((double)u0[i] - (double)u0[jp]);
+            pot += (u1(i) - u1(jp)) * (u0(i) - u0(jp));
             if (lo[ax] == 1) {
                 const int64_t jm = i - off[ax];
-                pot += ((double)u1[i] - (double)u1[jm]) * ((double)u0[i] - (double)u0[jm]);
+                pot += (u1(i) - u1(jm)) * (u0(i) - u0(jm));
             }
         }
         acc += 0.5 * lambda2 * pot;
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
+// FP16 level -> FP32 values (reads of the field by the host).
+__global__ void k_decode(const __half* in, float* out, int64_t n, float inv) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = __half2float(in[i]) * inv;
 }
 
 // ---------------------------------------------------------------------------
@@ -829,7 +1030,11 @@ struct Engine::Impl {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    DBuf<float> fields;  // 3 * batch * vol
+    DBuf<float> fields;  // 3 * batch * vol values (FP32, or FP16 in half the floats)
+    DBuf<uint32_t> f16_mx;   // FP16 storage: level maxima [batch][5]
+    DBuf<float> f16_smax;    // FP16 storage: largest |source sample| per member
+    std::vector<float> smax_host;
+    DBuf<float> decoded;     // FP16 storage: one decoded level for host reads
     DBuf<int32_t> lrs_cell;
     DBuf<uint32_t> lrs_info;
     DBuf<float> lrs_in, lrs_out;
@@ -873,6 +1078,16 @@ struct Engine::Impl {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     bool ref() const { return prm.mode == AFD_MODE_REF; }
+    bool f16() const { return prm.storage == AFD_STORE_FP16; }
+    // scale of level L of member b from the device maxima (host copy of the
+    // rule the kernels apply)
+    float host_level_scale(int32_t b, long long L) {
+        uint32_t m = 0;
+        float smax = 0.0f;
+        CK(cudaMemcpy(&m, f16_mx.ptr + (size_t)b * 5 + max_slot(L - 2), 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&smax, f16_smax.ptr + b, 4, cudaMemcpyDeviceToHost));
+        return level_scale(m, smax);
+    }
     float lambda2() const {
         const float t = prm.dt * prm.c / prm.dx;
         return t * t;
@@ -905,6 +1120,8 @@ struct Engine::Impl {
     void ensure_receivers(int64_t t_end);
     void build_args();
     void launch_step(int j, bool profile);
+    template <typename T>
+    void launch_step_t(int j, bool profile);
     int64_t kernels_per_step() const;
     void launch_step_count_only(int64_t n) { launches += kernels_per_step() * n + 1; }
     cudaGraphExec_t graph_for(int64_t n);
@@ -929,7 +1146,11 @@ void Engine::Impl::init_device() {
     if (vol * 3 > (int64_t)1 << 31 && vol > ((int64_t)1 << 31) - 1)
         throw Error(AFD_ERR_ARG, "grid too large for 32-bit cell indices");
     CK(cudaSetDevice(device));
-    fields.alloc((size_t)vol * 3 * prm.batch);
+    fields.alloc((size_t)vol * 3 * prm.batch / (f16() ? 2 : 1));  // vol is a multiple of 32
+    if (f16()) {
+        f16_mx.alloc((size_t)prm.batch * 5);
+        if (!f16_smax.ptr) f16_smax.alloc((size_t)prm.batch);
+    }
 
     tiles_x = (nx + FT_X - 1) / FT_X;
     tiles_y = (ny + FT_Y - 1) / FT_Y;
@@ -980,13 +1201,16 @@ void Engine::Impl::init_device() {
         CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
         if (!fn || q != cudaDriverEntryPointSuccess) throw Error(AFD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
         EncodeFn enc = (EncodeFn)fn;
+        const cuuint64_t es = f16() ? 2 : 4;
+        const CUtensorMapDataType dt = f16() ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
         const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)(3 * prm.batch * nz)};
-        const cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)plane * 4};
-        const cuuint32_t box_h[3] = {FH_X, FH_Y, 1}, box_o[3] = {FT_X, FT_Y, 1}, estr[3] = {1, 1, 1};
-        CUresult r1 = enc(&tm_halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, fields.ptr, dims, strides, box_h, estr,
+        const cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)plane * es};
+        const cuuint32_t box_h[3] = {(cuuint32_t)(f16() ? Tile<__half>::HX : Tile<float>::HX), FH_Y, 1},
+                         box_o[3] = {FT_X, FT_Y, 1}, estr[3] = {1, 1, 1};
+        CUresult r1 = enc(&tm_halo, dt, 3, fields.ptr, dims, strides, box_h, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        CUresult r2 = enc(&tm_own, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, fields.ptr, dims, strides, box_o, estr,
+        CUresult r2 = enc(&tm_own, dt, 3, fields.ptr, dims, strides, box_o, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) throw Error(AFD_ERR_CUDA, "tensor map encoding failed");
@@ -1003,8 +1227,10 @@ void Engine::Impl::build_fused() {
     F.tiles_x = tiles_x;
     F.tiles_y = tiles_y;
     int per_sm = 0;
-    CK(cudaFuncSetAttribute((const void*)k_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_stream, F_THREADS, F_SMEM));
+    const void* kern = f16() ? (const void*)k_stream<__half> : (const void*)k_stream<float>;
+    const size_t smem = f16() ? Tile<__half>::SMEM : Tile<float>::SMEM;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, F_THREADS, smem));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int64_t resident = (int64_t)std::max(per_sm, 1) * sms;
@@ -1172,6 +1398,12 @@ void Engine::Impl::upload_sources() {
         }
     }
     begin[(size_t)prm.batch] = (int32_t)cell.size();
+    if (f16()) {
+        smax_host.assign((size_t)prm.batch, 0.0f);
+        for (const Source& s : sources)
+            for (float v : s.sig) smax_host[(size_t)s.batch] = std::max(smax_host[(size_t)s.batch], std::fabs(v));
+        f16_smax.upload(smax_host);
+    }
     src_cell.upload(cell);
     src_begin.upload(begin);
     src_off.upload(off);
@@ -1218,7 +1450,13 @@ void Engine::Impl::build_args() {
     a.g = GridDev{nx, ny, nz, pitch, plane, vol};
     a.batch = prm.batch;
     a.mode = prm.mode;
-    for (int k = 0; k < 3; ++k) a.p[k] = fields.ptr + (size_t)k * vol * prm.batch;
+    if (f16()) {
+        for (int k = 0; k < 3; ++k) a.f16.h[k] = reinterpret_cast<__half*>(fields.ptr) + (size_t)k * vol * prm.batch;
+        a.f16.mx = f16_mx.ptr;
+        a.f16.src_max = f16_smax.ptr;
+    } else {
+        for (int k = 0; k < 3; ++k) a.p[k] = fields.ptr + (size_t)k * vol * prm.batch;
+    }
     a.d_step = d_step.ptr;
     a.lambda2 = lambda2();
     a.cint = 2.0f * (1.0f - 3.0f * a.lambda2);
@@ -1298,8 +1536,14 @@ enum KernelKind { KK_INTERIOR, KK_LRS, KK_PML_AUX, KK_PML_P, KK_SRC_RCV, KK_FUSE
 static const char* kKernelNames[KK_COUNT] = {"interior", "boundary", "pml_aux", "pml_pressure",
                                              "source_receiver", "interior_stream"};
 
-// One time step, global step = *d_step + j (simulation.hpp:358-392).
 void Engine::Impl::launch_step(int j, bool profile) {
+    if (f16()) launch_step_t<__half>(j, profile);
+    else launch_step_t<float>(j, profile);
+}
+
+// One time step, global step = *d_step + j (simulation.hpp:358-392).
+template <typename T>
+void Engine::Impl::launch_step_t(int j, bool profile) {
     const StepArgs& a = args;
     auto begin = [&](int kind) {
         if (!profile) return;
@@ -1319,28 +1563,32 @@ void Engine::Impl::launch_step(int j, bool profile) {
     const dim3 blk(64, 4, 1);
     if (use_fused()) {
         begin(KK_FUSED);
-        k_stream<<<fused_grid, F_THREADS, F_SMEM, stream>>>(tm_halo, tm_own, a, fdev, j);
+        k_stream<T><<<fused_grid, F_THREADS, Tile<T>::SMEM, stream>>>(tm_halo, tm_own, a, fdev, j);
         end();
         ++launches;
     } else {
         const dim3 grd((unsigned)((nx - 2 + 63) / 64), (unsigned)((ny - 2 + 3) / 4),
                        (unsigned)((nz - 2) * prm.batch));
         begin(KK_INTERIOR);
-        k_interior<<<grd, blk, 0, stream>>>(a, j);
+        k_interior<T><<<grd, blk, 0, stream>>>(a, j);
         end();
         ++launches;
     }
     if (a.lrs.n > 0) {
         const dim3 grd((unsigned)((a.lrs.n + 255) / 256), (unsigned)prm.batch);
         begin(KK_LRS);
-        if (ref()) launch_lrs<true>(a, j, grd, stream);
-        else launch_lrs<false>(a, j, grd, stream);
+        if constexpr (sizeof(T) == 4) {
+            if (ref()) launch_lrs<true, float>(a, j, grd, stream);
+            else launch_lrs<false, float>(a, j, grd, stream);
+        } else {
+            launch_lrs<false, T>(a, j, grd, stream);
+        }
         end();
         ++launches;
     }
     if (a.pml.width > 0) {
         if (ref()) {
-            if (nx > 4 && ny > 4 && nz > 4) {
+            if (sizeof(T) == 4 && nx > 4 && ny > 4 && nz > 4) {
                 const dim3 grd((unsigned)((nx - 4 + 63) / 64), (unsigned)((ny - 4 + 3) / 4),
                                (unsigned)((nz - 4) * prm.batch));
                 begin(KK_PML_AUX);
@@ -1364,8 +1612,8 @@ void Engine::Impl::launch_step(int j, bool profile) {
                 dim3 grd, blk;
                 shape(bx, grd, blk);
                 begin(KK_PML_P);
-                if (psi) k_pml_box_p<true><<<grd, blk, 0, stream>>>(a, bx, j);
-                else k_pml_box_p<false><<<grd, blk, 0, stream>>>(a, bx, j);
+                if (psi) k_pml_box_p<true, T><<<grd, blk, 0, stream>>>(a, bx, j);
+                else k_pml_box_p<false, T><<<grd, blk, 0, stream>>>(a, bx, j);
                 end();
                 ++launches;
             }
@@ -1375,14 +1623,14 @@ void Engine::Impl::launch_step(int j, bool profile) {
                     shape(bx, grd, blk);
                     begin(KK_PML_AUX);
                     if (ax == 0) {
-                        if (psi) k_pml_box_aux<0, true><<<grd, blk, 0, stream>>>(a, bx, j);
-                        else k_pml_box_aux<0, false><<<grd, blk, 0, stream>>>(a, bx, j);
+                        if (psi) k_pml_box_aux<0, true, T><<<grd, blk, 0, stream>>>(a, bx, j);
+                        else k_pml_box_aux<0, false, T><<<grd, blk, 0, stream>>>(a, bx, j);
                     } else if (ax == 1) {
-                        if (psi) k_pml_box_aux<1, true><<<grd, blk, 0, stream>>>(a, bx, j);
-                        else k_pml_box_aux<1, false><<<grd, blk, 0, stream>>>(a, bx, j);
+                        if (psi) k_pml_box_aux<1, true, T><<<grd, blk, 0, stream>>>(a, bx, j);
+                        else k_pml_box_aux<1, false, T><<<grd, blk, 0, stream>>>(a, bx, j);
                     } else {
-                        if (psi) k_pml_box_aux<2, true><<<grd, blk, 0, stream>>>(a, bx, j);
-                        else k_pml_box_aux<2, false><<<grd, blk, 0, stream>>>(a, bx, j);
+                        if (psi) k_pml_box_aux<2, true, T><<<grd, blk, 0, stream>>>(a, bx, j);
+                        else k_pml_box_aux<2, false, T><<<grd, blk, 0, stream>>>(a, bx, j);
                     }
                     end();
                     ++launches;
@@ -1391,8 +1639,8 @@ void Engine::Impl::launch_step(int j, bool profile) {
     }
     if (a.src.n > 0 || a.rcv.n > 0) {
         begin(KK_SRC_RCV);
-        if (inline_ok) k_src_rcv_inline<<<(unsigned)prm.batch, 256, 0, stream>>>(a, inl, j);
-        else k_src_rcv<<<(unsigned)prm.batch, 128, 0, stream>>>(a, j, 1, 1);
+        if (inline_ok) k_src_rcv_inline<T><<<(unsigned)prm.batch, 256, 0, stream>>>(a, inl, j);
+        else k_src_rcv<T><<<(unsigned)prm.batch, 128, 0, stream>>>(a, j, 1, 1);
         end();
         ++launches;
     }
@@ -1471,7 +1719,9 @@ Engine::Engine(const afd_params& p) : d_(new Impl) {
         throw Error(AFD_ERR_ARG, "dx, c and dt must be positive");
     if (p.batch < 1 || p.batch > 4096) throw Error(AFD_ERR_ARG, "batch must be in 1..4096");
     if (p.mode != AFD_MODE_REF && p.mode != AFD_MODE_FIXED) throw Error(AFD_ERR_ARG, "unknown mode");
-    if (p.storage != AFD_STORE_FP32) throw Error(AFD_ERR_ARG, "unsupported storage");
+    if (p.storage != AFD_STORE_FP32 && p.storage != AFD_STORE_FP16) throw Error(AFD_ERR_ARG, "unsupported storage");
+    if (p.storage == AFD_STORE_FP16 && p.mode != AFD_MODE_FIXED)
+        throw Error(AFD_ERR_ARG, "FP16 storage requires the FIXED scheme");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         throw Error(AFD_ERR_CUDA, "no CUDA device available");
@@ -1680,8 +1930,9 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
             }
             if (flag && D.prm.watchdog) {
                 D.steps_done += i;
-                throw Error(AFD_ERR_NUMERIC, "pressure left the finite bound |p| < 1e30 by step " +
-                                                 std::to_string(D.steps_done));
+                throw Error(AFD_ERR_NUMERIC, std::string(D.f16() ? "pressure left the FP16 storage range"
+                                                                 : "pressure left the finite bound |p| < 1e30") +
+                                                 " by step " + std::to_string(D.steps_done));
             }
             if (cb && cb(last, steps, user) != 0) {
                 status = AFD_ERR_ABORTED;
@@ -1701,8 +1952,9 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     D.steps_done += i;
     if (flag & 2) throw Error(AFD_ERR_CUDA, "step kernel pipeline wait timed out");
     if (flag && D.prm.watchdog)
-        throw Error(AFD_ERR_NUMERIC,
-                    "pressure left the finite bound |p| < 1e30 by step " + std::to_string(D.steps_done));
+        throw Error(AFD_ERR_NUMERIC, std::string(D.f16() ? "pressure left the FP16 storage range"
+                                                         : "pressure left the finite bound |p| < 1e30") +
+                                         " by step " + std::to_string(D.steps_done));
     if (status == AFD_OK && cb) cb(steps, steps, user);
     return status;
 }
@@ -1754,6 +2006,18 @@ void Engine::update_source(int64_t index, int64_t t0, const float* sig, int64_t 
         D.src_dirty = true;
         return;
     }
+    if (D.f16() && D.f16_smax.ptr && (size_t)s.batch < D.smax_host.size()) {
+        // the scale rule's source maximum follows larger new samples from
+        // the next queued step on
+        float& cur = D.smax_host[(size_t)s.batch];
+        float m = cur;
+        for (int64_t k = 0; k < len; ++k) m = std::max(m, std::fabs(sig[k]));
+        if (m > cur) {
+            cur = m;
+            CK(cudaSetDevice(D.device));
+            CK(cudaMemcpyAsync(D.f16_smax.ptr + s.batch, &cur, 4, cudaMemcpyHostToDevice, D.stream));
+        }
+    }
     // device position of this source: sources are stored grouped by batch member
     int64_t off = 0;
     for (int32_t b = 0; b < D.prm.batch; ++b)
@@ -1769,10 +2033,20 @@ void Engine::update_source(int64_t index, int64_t t0, const float* sig, int64_t 
         }
 }
 
+// The newest level of one member as FP32 values on the device (FP16
+// storage: decoded into a scratch buffer).
 static const float* latest_field(Engine::Impl& D, int32_t batch) {
     if (D.steps_done == 0) return nullptr;
     const long long g = D.steps_done - 1;
-    return D.fields.ptr + (size_t)buf_new(g) * D.vol * D.prm.batch + (size_t)batch * D.vol;
+    if (!D.f16()) return D.fields.ptr + (size_t)buf_new(g) * D.vol * D.prm.batch + (size_t)batch * D.vol;
+    const __half* h = reinterpret_cast<const __half*>(D.fields.ptr) + (size_t)buf_new(g) * D.vol * D.prm.batch +
+                      (size_t)batch * D.vol;
+    if (D.decoded.n != (size_t)D.vol) D.decoded.alloc((size_t)D.vol);
+    const float inv = 1.0f / D.host_level_scale(batch, g);
+    k_decode<<<1184, 256, 0, D.stream>>>(h, D.decoded.ptr, D.vol, inv);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(D.stream));
+    return D.decoded.ptr;
 }
 
 void Engine::get_field(int32_t batch, float* out, int64_t cap) {
@@ -1871,13 +2145,21 @@ double Engine::energy(int32_t batch) {
     const long long g = D.steps_done - 1;
     const size_t base = (size_t)batch * D.vol;
     const size_t stride = (size_t)D.vol * D.prm.batch;
-    const float* u1 = D.fields.ptr + (size_t)buf_new(g) * stride + base;
-    const float* u0 = D.fields.ptr + (size_t)buf_cur(g) * stride + base;
     CK(cudaMemsetAsync(D.d_energy.ptr, 0, sizeof(double), D.stream));
     const dim3 blk(64, 4, 1);
     const dim3 grd((unsigned)((D.nx - 2 + 63) / 64), (unsigned)((D.ny - 2 + 3) / 4), (unsigned)(D.nz - 2));
-    k_energy<<<grd, blk, 0, D.stream>>>(u1, u0, GridDev{D.nx, D.ny, D.nz, D.pitch, D.plane, D.vol},
-                                        (double)D.lambda2(), D.d_energy.ptr);
+    const GridDev gd{D.nx, D.ny, D.nz, D.pitch, D.plane, D.vol};
+    if (D.f16()) {
+        const __half* h = reinterpret_cast<const __half*>(D.fields.ptr);
+        const float inv1 = 1.0f / D.host_level_scale(batch, g), inv0 = 1.0f / D.host_level_scale(batch, g - 1);
+        k_energy<__half><<<grd, blk, 0, D.stream>>>(h + (size_t)buf_new(g) * stride + base,
+                                                    h + (size_t)buf_cur(g) * stride + base, inv1, inv0, gd,
+                                                    (double)D.lambda2(), D.d_energy.ptr);
+    } else {
+        k_energy<float><<<grd, blk, 0, D.stream>>>(D.fields.ptr + (size_t)buf_new(g) * stride + base,
+                                                   D.fields.ptr + (size_t)buf_cur(g) * stride + base, 1.0f, 1.0f,
+                                                   gd, (double)D.lambda2(), D.d_energy.ptr);
+    }
     CK(cudaGetLastError());
     double e = 0.0;
     CK(cudaMemcpyAsync(&e, D.d_energy.ptr, sizeof(double), cudaMemcpyDeviceToHost, D.stream));

@@ -35,6 +35,27 @@ constexpr int F_THREADS = F_CONSUMERS + 32;
 constexpr size_t F_SMEM = (size_t)F_STAGES * F_STAGE_BYTES + 2 * F_STAGES * 8 + F_STAGES * 4 + 128;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s
 
+// Stage layout per storage type. FP16 levels: the halo box starts 8 cells
+// before the tile (x times 2 bytes stays a multiple of 16) and is 80 cells
+// wide; 4.9 KB of each 5 KB stage is copied.
+template <typename T>
+struct Tile;
+template <>
+struct Tile<float> {
+    static constexpr int HX = FH_X, XOFF = 4, PN_PAD = F_PN_PAD, STAGE = F_STAGE_BYTES, TX = F_TX_BYTES;
+    static constexpr size_t SMEM = F_SMEM;
+};
+template <>
+struct Tile<__half> {
+    static constexpr int HX = FT_X + 16, XOFF = 8;
+    static constexpr int PN_BYTES = HX * FH_Y * 2;                               // 2880
+    static constexpr int PN_PAD = (PN_BYTES + 127) / 128 * 128;                  // 2944
+    static constexpr int PO_BYTES = FT_X * FT_Y * 2;                             // 2048
+    static constexpr int STAGE = (PN_PAD + PO_BYTES + 127) / 128 * 128;          // 5120
+    static constexpr int TX = PN_BYTES + PO_BYTES;                               // 4928
+    static constexpr size_t SMEM = (size_t)F_STAGES * STAGE + 2 * F_STAGES * 8 + F_STAGES * 4 + 128;
+};
+
 // Work decomposition of the streaming kernel.
 struct FusedDev {
     int32_t tiles_x, tiles_y, dz, n_chunks;

@@ -6,7 +6,8 @@
 //
 // Additions, all optional and before `sd`/`sdt` (they set the parameters of
 // the next simulation): `mode ref|fixed`, `dx <m>`, `c <m/s>`, `dt <s>`,
-// `fs <Hz>`, `pmlfaces <mask>`, `graphs 0|1`. `vis` is headless: it records
+// `fs <Hz>`, `pmlfaces <mask>`, `graphs 0|1`, `precision fp32|fp16` (FP16
+// field storage, with `mode fixed`). `vis` is headless: it records
 // the y level; `visdump <file>` writes that plane of the latest field as
 // text rows.
 #include <unistd.h>
@@ -330,6 +331,11 @@ struct Repl {
         add("c", {"float"}, [this](const std::vector<std::string>& a) { parse_float(a[0], &prm.c); });
         add("dt", {"float"}, [this](const std::vector<std::string>& a) { parse_float(a[0], &prm.dt); });
         add("fs", {"float"}, [this](const std::vector<std::string>& a) { parse_float(a[0], &prm.fs); });
+        add("precision", {"string"}, [this](const std::vector<std::string>& a) {
+            if (a[0] == "fp32") prm.storage = AFD_STORE_FP32;
+            else if (a[0] == "fp16") prm.storage = AFD_STORE_FP16;
+            else std::cout << "Valid command arguments are 'fp32' or 'fp16'\n";
+        });
         add("graphs", {"int"}, [this](const std::vector<std::string>& a) {
             int v = 1;
             parse_int(a[0], &v);

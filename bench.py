@@ -41,6 +41,8 @@ def parse():
                     help="NX,NY,NZ: the same construction at another size (profiling captures)")
     ap.add_argument("--legs", default="device,e2e,roofline,cpu",
                     help="comma list of device,e2e,roofline,cpu")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
+                    help="field storage: fp32, or fp16 levels with per-level power-of-two scales")
     return ap.parse_args()
 
 
@@ -176,9 +178,13 @@ def main():
     nx, ny, nz = cfg.dims
     interior = (nx - 2) * (ny - 2) * (nz - 2)
     metric = "Mcell-updates/s"
-    config = {"workload": "%dx%dx%d single-source FP32 (4 materials K=4, 20 boxes, PML x+/z+ "
-                          "width 12, 32 receivers)" % (nx, ny, nz), "grid": [nx, ny, nz], "interior_cells": interior,
-              "mode": "FIXED", "l2_flush": "not needed: three 252 MB field levels exceed the 126 MB L2",
+    f16 = args.storage == "fp16"
+    lvl_mb = interior * (2 if f16 else 4) / 1e6
+    config = {"workload": "%dx%dx%d single-source %s (4 materials K=4, 20 boxes, PML x+/z+ "
+                          "width 12, 32 receivers)" % (nx, ny, nz, "FP16-storage" if f16 else "FP32"),
+              "grid": [nx, ny, nz], "interior_cells": interior, "mode": "FIXED", "storage": args.storage,
+              "l2_flush": "not needed: three %.0f MB field levels exceed the 126 MB L2" % lvl_mb
+              if 3 * lvl_mb > 126 else "none: the field levels fit in L2 (L2-resident workload)",
               "parallelism": "replicas" if world > 1 else "single"}
 
     if args.impl == "reference":
@@ -204,7 +210,7 @@ def main():
 
     def make_sim(profile=0, graphs=1):
         sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, device=local, profile=profile,
-                             graphs=graphs)
+                             graphs=graphs, storage=1 if f16 else 0)
         sim.SetModel(pkg.Model.from_voxels(cfg.vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
         sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi)
         sim.AddSourceCell(cfg.sources[0][0], cfg.sources[0][1])
@@ -241,7 +247,7 @@ def main():
         line["e2e"] = e2e_leg(sim, cfg, K, interior, world, metric)
     sim.close()
     if "roofline" in legs:
-        line["roofline"] = roofline_leg(make_sim, K, interior)
+        line["roofline"] = roofline_leg(make_sim, K, interior, 6.0 if f16 else 12.0)
     if rank == 0 and world == 1 and "cpu" in legs and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(cfg, 4)
     if rank == 0:
@@ -275,8 +281,10 @@ def e2e_leg(sim, cfg, K, interior, world, metric):
             "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * len(cfg.receivers)}
 
 
-def roofline_leg(make_sim, K, interior):
-    """Roofline of the dominant kernel from per-launch CUDA events."""
+def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0):
+    """Roofline of the dominant kernel from per-launch CUDA events. The
+    interior kernel moves bytes_per_cell per interior cell: read p^n, read
+    p^{n-1}, write p^{n+1} (4-byte values, or 2-byte FP16 storage)."""
     psim = make_sim(profile=1, graphs=0)
     psim.Run(min(K, 400) + 1)
     stats = psim.kernel_stats()
@@ -284,14 +292,14 @@ def roofline_leg(make_sim, K, interior):
     top = max(stats.items(), key=lambda kv: kv[1][1])
     name, (n_launch, tot_ms) = top
     avg_ms = tot_ms / max(n_launch, 1)
-    step_kernel_bytes = 12.0 * interior  # read p^n, read p^{n-1}, write p^{n+1}
+    step_kernel_bytes = bytes_per_cell * interior
     peak, peak_kind = peaks()
     achieved = step_kernel_bytes / (avg_ms / 1e3) / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile)).get(name)
+            traffic = json.load(open(tfile)).get(name + ("_fp16" if bytes_per_cell < 12 else ""))
         except Exception:
             traffic = None
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_kind,

@@ -23,7 +23,11 @@
  * -ffp-contract=off the FP32 build rounds exactly as the kernels specify.
  *
  * The same source compiled with -DORA_REAL=double is the FP64 version of
- * each scheme.
+ * each scheme. The FP32 build also exports ora_simulate_f16, the FIXED
+ * scheme with FP16 field storage (the engine's AFD_STORE_FP16 option, which
+ * has no counterpart in the reference): FP32 arithmetic on values that are
+ * rounded to binary16 times a power-of-two scale whenever a pressure level
+ * is stored, the scale of each level chosen by level_scale() below.
  *
  * Parity of this restatement is pinned against the reference's own kernel
  * sources compiled in oracle/ref_harness.c (outputs under oracle/_ref/).
@@ -37,6 +41,55 @@
 #define ORA_REAL float
 #endif
 typedef ORA_REAL real;
+
+/* ---- FP16 storage ------------------------------------------------------
+ * IEEE 754 binary32 -> binary16 with round to nearest even, and back. */
+static inline uint16_t f32_to_f16(float f) {
+    uint32_t x;
+    memcpy(&x, &f, 4);
+    const uint32_t sign = (x >> 16) & 0x8000u, ax = x & 0x7fffffffu;
+    if (ax > 0x7f800000u) return (uint16_t)(sign | 0x7e00u);     /* NaN */
+    if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);    /* >= 65520 rounds to inf */
+    if (ax < 0x38800000u) {                                      /* below 2^-14: subnormal */
+        float a;
+        memcpy(&a, &ax, 4);
+        return (uint16_t)(sign | (uint32_t)rintf(a * 16777216.0f)); /* units of 2^-24 */
+    }
+    const uint32_t r = ax + 0x0fffu + ((ax >> 13) & 1u);         /* round the low 13 bits */
+    return (uint16_t)(sign | ((r - (112u << 23)) >> 13));        /* rebias 127 -> 15 */
+}
+
+static inline float f16_to_f32(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    uint32_t x;
+    float r;
+    if (e == 0) {
+        r = (float)m * 5.9604644775390625e-8f;                   /* m * 2^-24, exact */
+        return sign ? -r : r;
+    }
+    x = sign | (e == 31 ? 0x7f800000u | (m << 13) : ((e + 112u) << 23) | (m << 13));
+    memcpy(&r, &x, 4);
+    return r;
+}
+
+/* The value a stored level holds: v * s rounded to binary16, times 1/s. */
+static inline float q16(float v, float s, float inv) { return f16_to_f32(f32_to_f16(v * s)) * inv; }
+
+/* Scale of the level written at step g: 2^(10 - e) with 2^e above the
+ * largest magnitude m of level g - 2 (the last level complete when the
+ * step starts, other than the one it reads as p^n) and of the batch
+ * member's source samples smax; 1 when both are zero; exponent clamped to
+ * [-60, 60]. Two steps of the scheme grow a field by far less than the
+ * 2^6 headroom this leaves below the binary16 maximum. */
+static float level_scale(float m, float smax) {
+    const float a = m > smax ? m : smax;
+    if (!(a > 0.0f)) return 1.0f;
+    int e;
+    frexpf(a, &e);
+    int k = 10 - e;
+    k = k > 60 ? 60 : (k < -60 ? -60 : k);
+    return ldexpf(1.0f, k);
+}
 
 #ifndef ORA_NAME
 #define ORA_NAME ora_simulate_f32
@@ -275,13 +328,20 @@ static void pml_aux(int mode, const PmlK* K, unsigned axes, const real* pnew, co
  *   last level or NULL.
  * Returns 0, or -1 on bad input / unphysical geometry, -2 on no memory.
  */
-int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int32_t* vox, int nmat,
-             int K, const double* a, const double* b, double dx, double c, double dt, int pml_width,
-             unsigned faces, const float* ksi_x, const float* ksi_y, const float* ksi_z, int nsrc,
-             const int32_t* src_ijk, const int64_t* src_off, const int64_t* src_len,
-             const float* src_data, int nrcv, const int32_t* rcv_ijk, int n_runs,
-             const int64_t* run_steps, float* rcv_out, float* field_out) {
+static int simulate(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int32_t* vox, int nmat,
+                    int K, const double* a, const double* b, double dx, double c, double dt, int pml_width,
+                    unsigned faces, const float* ksi_x, const float* ksi_y, const float* ksi_z, int nsrc,
+                    const int32_t* src_ijk, const int64_t* src_off, const int64_t* src_len,
+                    const float* src_data, int nrcv, const int32_t* rcv_ijk, int n_runs,
+                    const int64_t* run_steps, float* rcv_out, float* field_out, int f16) {
     if (nx < 3 || ny < 3 || nz < 3 || K < 1 || (mx && (mx > nx || my > ny || mz > nz))) return -1;
+    if (f16 && (mode != 1 || sizeof(real) != sizeof(float))) return -1;
+    float smax = 0.0f;
+    for (int s = 0; s < nsrc; ++s)
+        for (int64_t k = 0; k < src_len[s]; ++k) {
+            const float v = fabsf(src_data[src_off[s] + k]);
+            smax = v > smax ? v : smax;
+        }
     const int64_t pitch = nx, plane = (int64_t)nx * ny, vol = plane * nz;
     int64_t total = 0;
     for (int r = 0; r < n_runs; ++r) total += run_steps[r];
@@ -371,8 +431,18 @@ int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
             const int w = (int)((2 + 2 * (g % 3)) % 3);
             real* pn = P[w];
             const real* pc = P[(w + 1) % 3];
-            const real* po = P[(w + 2) % 3];
-            /* leapfrog.cl:40-53 */
+            real* po = P[(w + 2) % 3];
+            float sp = 1.0f, isp = 1.0f;
+            if (f16) {
+                float m = 0.0f;
+#pragma omp parallel for schedule(static) reduction(max : m)
+                for (int64_t i = 0; i < vol; ++i) m = fabsf(po[i]) > m ? fabsf(po[i]) : m;
+                sp = level_scale(m, smax);
+                isp = 1.0f / sp;
+            }
+            /* leapfrog.cl:40-53; FP16 storage evaluates the same update as
+             * p + ((p - p^{n-1}) + lambda^2 (S - 6p)), the increment formed
+             * before it meets the stored level */
 #pragma omp parallel for schedule(static)
             for (int z = 1; z <= nz - 2; ++z)
                 for (int y = 1; y <= ny - 2; ++y)
@@ -383,7 +453,10 @@ int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
                         s = s + pc[i - pitch];
                         s = s + pc[i + plane];
                         s = s + pc[i - plane];
-                        pn[i] = lambda2 * s + cint * pc[i] - po[i];
+                        if (!f16)
+                            pn[i] = lambda2 * s + cint * pc[i] - po[i];
+                        else
+                            pn[i] = pc[i] + ((pc[i] - po[i]) + lambda2 * (s - (real)6.0f * pc[i]));
                     }
             /* simulation.hpp:365 */
             const int ix_buf = K - 1 - (int)(g % K);
@@ -437,6 +510,24 @@ int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
                         psiph[i] = ps;
                         pn[i] = pv;
                     }
+                }
+            }
+            if (f16) {
+                /* the store of the new level to the FP16 grid of scale sp */
+#pragma omp parallel for schedule(static)
+                for (int z = 1; z <= nz - 2; ++z)
+                    for (int y = 1; y <= ny - 2; ++y)
+                        for (int x = 1; x <= nx - 2; ++x) {
+                            const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
+                            pn[i] = q16(pn[i], sp, isp);
+                        }
+            }
+            if (pml_width > 0 && mode == 1) {
+                const int lv = (int)((g + 1) & 1);
+                real* fx = fi[0][lv]; real* fy = fi[1][lv]; real* fz = fi[2][lv];
+                const real* fx1 = fi[0][lv ^ 1]; const real* fy1 = fi[1][lv ^ 1]; const real* fz1 = fi[2][lv ^ 1];
+                real* psiph = psi[lv];
+                {
 #pragma omp parallel for schedule(static)
                     for (int64_t e = 0; e < npml; ++e) {
                         const int64_t i = pml_cells[e];
@@ -451,7 +542,7 @@ int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
                 const int64_t i = (int64_t)src_ijk[3 * s + 2] * plane + (int64_t)src_ijk[3 * s + 1] * pitch +
                                   src_ijk[3 * s];
                 const real v = (g < src_len[s]) ? (real)src_data[src_off[s] + g] : (real)0.0f;
-                pn[i] += v;
+                pn[i] = f16 ? q16(pn[i] + v, sp, isp) : pn[i] + v;
             }
             /* mic.cl:32-41 */
             for (int m = 0; m < nrcv; ++m) {
@@ -491,3 +582,38 @@ int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
     free(pml_flags);
     return 0;
 }
+
+int ORA_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int32_t* vox, int nmat,
+             int K, const double* a, const double* b, double dx, double c, double dt, int pml_width,
+             unsigned faces, const float* ksi_x, const float* ksi_y, const float* ksi_z, int nsrc,
+             const int32_t* src_ijk, const int64_t* src_off, const int64_t* src_len,
+             const float* src_data, int nrcv, const int32_t* rcv_ijk, int n_runs,
+             const int64_t* run_steps, float* rcv_out, float* field_out) {
+    return simulate(mode, nx, ny, nz, mx, my, mz, vox, nmat, K, a, b, dx, c, dt, pml_width, faces, ksi_x,
+                    ksi_y, ksi_z, nsrc, src_ijk, src_off, src_len, src_data, nrcv, rcv_ijk, n_runs, run_steps,
+                    rcv_out, field_out, 0);
+}
+
+#ifndef ORA_NO_F16
+/* The storage rounding and the level scale rule, for the tests that pin
+ * them: out[i] = q16(in[i], s, 1/s); scales[i] = level_scale(m[i], smax). */
+void ora_f16_round(const float* in, float* out, int64_t n, float s) {
+    for (int64_t i = 0; i < n; ++i) out[i] = q16(in[i], s, 1.0f / s);
+}
+
+void ora_level_scale(const float* m, float* scales, int64_t n, float smax) {
+    for (int64_t i = 0; i < n; ++i) scales[i] = level_scale(m[i], smax);
+}
+
+/* FIXED scheme with FP16 storage of the three pressure levels. */
+int ora_simulate_f16(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int32_t* vox, int nmat,
+                     int K, const double* a, const double* b, double dx, double c, double dt, int pml_width,
+                     unsigned faces, const float* ksi_x, const float* ksi_y, const float* ksi_z, int nsrc,
+                     const int32_t* src_ijk, const int64_t* src_off, const int64_t* src_len,
+                     const float* src_data, int nrcv, const int32_t* rcv_ijk, int n_runs,
+                     const int64_t* run_steps, float* rcv_out, float* field_out) {
+    return simulate(mode, nx, ny, nz, mx, my, mz, vox, nmat, K, a, b, dx, c, dt, pml_width, faces, ksi_x,
+                    ksi_y, ksi_z, nsrc, src_ijk, src_off, src_len, src_data, nrcv, rcv_ijk, n_runs, run_steps,
+                    rcv_out, field_out, 1);
+}
+#endif

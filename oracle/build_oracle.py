@@ -1,7 +1,7 @@
 """Builds the CPU oracle (test infrastructure, never the product path).
 
   _build/liboracle.so   the restatement afd_oracle.c, FP32 and FP64 entry
-                        points (ora_simulate_f32 / ora_simulate_f64)
+                        points (ora_simulate_f32 / ora_simulate_f64 / ora_simulate_f16)
   _ref/libref32.so      the reference's own kernel sources compiled from
   _ref/libref64.so      where they lie (ref_harness.c), FP32 and FP64
                         (ref_simulate_f32 / ref_simulate_f64); built only
@@ -42,7 +42,7 @@ def build_restatement(force=False):
         o32 = os.path.join(BUILD, "ora32.o")
         o64 = os.path.join(BUILD, "ora64.o")
         _cc(FLAGS + ["-c", src, "-o", o32])
-        _cc(FLAGS + ["-DORA_REAL=double", "-DORA_NAME=ora_simulate_f64", "-c", src, "-o", o64])
+        _cc(FLAGS + ["-DORA_REAL=double", "-DORA_NAME=ora_simulate_f64", "-DORA_NO_F16", "-c", src, "-o", o64])
         _cc(["-shared", "-fopenmp", o32, o64, "-o", out, "-lm"])
     return out
 

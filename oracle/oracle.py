@@ -55,6 +55,7 @@ def simulate(grid, vox=None, a=None, b=None, dx=0.02, c=340.0, dt=3.125e-5, mode
     """One batch member. grid = (nx, ny, nz); vox int32 [mz, my, mx] or None;
     a, b [nmat, K]; sources = [((i, j, k), signal)]; receivers = [(i, j, k)];
     runs = list of consecutive run lengths (default [steps]).
+    precision "f16": the FIXED scheme with FP16 storage of the pressure levels.
     Returns (receivers [n, T] float32, field [nz, ny, nx] or None)."""
     nx, ny, nz = grid
     runs = list(runs) if runs is not None else [steps]

@@ -51,6 +51,13 @@ def test_create_without_device_fails_cleanly(pkg):
     assert "no CUDA device" in str(ei.value)
 
 
+def test_fp16_storage_needs_fixed_scheme(pkg):
+    with pytest.raises(pkg.AfdError) as ei:
+        pkg.Simulation(mode=pkg.afd.MODE_REF, storage=pkg.afd.STORE_FP16)
+    assert ei.value.status == pkg.afd.ERR_ARG
+    assert "FIXED" in str(ei.value)
+
+
 # ---------------------------------------------------------------- classifier
 _MASKS = [1, 2, 4, 8, 16, 32, 5, 9, 17, 33, 6, 10, 18, 34, 20, 36, 24, 40, 21, 37, 25, 41, 22, 38, 26, 42]
 

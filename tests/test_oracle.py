@@ -80,3 +80,76 @@ def test_source_on_a_boundary_cell_persists_like_the_reference():
     if oracle.available("ref", "f32"):
         r2, _ = oracle.simulate(impl="ref", **inp)
         assert np.array_equal(rcv, r2)
+
+
+# ---------------------------------------------------------------- FP16 storage
+def _f16_lib():
+    import ctypes as C
+    lib = C.CDLL(oracle.ORA_LIB)
+    P = C.POINTER
+    lib.ora_f16_round.argtypes = [P(C.c_float), P(C.c_float), C.c_int64, C.c_float]
+    lib.ora_level_scale.argtypes = [P(C.c_float), P(C.c_float), C.c_int64, C.c_float]
+    return lib, C
+
+
+def test_f16_storage_rounding_matches_numpy():
+    """The restatement's binary16 round trip (round to nearest even, own
+    bit arithmetic) equals numpy's float32 -> float16 -> float32 on random
+    bit patterns, the overflow and subnormal edges, and with scales."""
+    lib, C = _f16_lib()
+    rng = np.random.default_rng(0)
+    x = rng.integers(0, 2**32, 1_000_000, dtype=np.uint64).astype(np.uint32).view(np.float32)
+    x = x[np.isfinite(x)]
+    edge = np.array([0.0, -0.0, 65504, 65519.99, 65520, 65536, 2**-14, 2**-24, 2**-25, 3 * 2**-26, -1e-8],
+                    np.float32)
+    x = np.concatenate([x, edge, np.arange(-70000, 70000, 0.37, dtype=np.float32)])
+    for s in (1.0, 2.0**-20, 2.0**13, 2.0**40):
+        out = np.empty_like(x)
+        lib.ora_f16_round(x.ctypes.data_as(C.POINTER(C.c_float)), out.ctypes.data_as(C.POINTER(C.c_float)),
+                          x.size, s)
+        with np.errstate(over="ignore"):
+            want = (x * np.float32(s)).astype(np.float16).astype(np.float32) * np.float32(1.0 / s)
+        same = (out == want) | (np.isnan(out) & np.isnan(want))
+        assert same.all(), (s, x[~same][:5])
+
+
+def test_level_scale_rule():
+    """2^(10 - e) with max(m, smax) < 2^e, clamped exponents, 1 for zero."""
+    import math
+    lib, C = _f16_lib()
+    m = np.array([0.0, 1.0, 0.75, 1024.0, 1e-30, 3e38, 2.0**-130, 5.0, 6e-5], np.float32)
+    for smax in (0.0, 0.5, 100.0):
+        out = np.empty_like(m)
+        lib.ora_level_scale(m.ctypes.data_as(C.POINTER(C.c_float)), out.ctypes.data_as(C.POINTER(C.c_float)),
+                            m.size, smax)
+        for v, s in zip(m, out):
+            a = max(float(v), smax)
+            if a == 0.0:
+                assert s == 1.0
+                continue
+            e = math.frexp(a)[1]
+            assert s == 2.0 ** max(-60, min(60, 10 - e))
+            assert a * s < 2.0 ** 10 or 10 - e < -60
+
+
+def test_fp16_storage_restatement_error():
+    """FP16 storage of the FIXED scheme on a small room with PML: within
+    -40 dB of the FP64 scheme, and FP32 within -80 dB."""
+    sys.path.insert(0, os.path.join(HERE, ".."))
+    import __graft_entry__ as ge
+    W = ge.load().workloads
+    rng = np.random.default_rng(3)
+    vox = W.room(40, 34, 30, 63 & ~W.FACE_ZP, n_boxes=1, nmat=2, seed=4, box_min=4, box_max=8)
+    a, b = W.passive_filters(2, 2, 5)
+    ksi = W.ksi_arrays((40, 34, 30), 8, W.FACE_ZP)
+    sig = W.gaussian_pulse(600, 24000.0)
+    kw = dict(grid=(40, 34, 30), vox=vox, a=a, b=b, dx=0.025, c=343.0, dt=W.courant_dt(0.025, 343.0), mode=1,
+              pml_width=8, faces=W.FACE_ZP, ksi=ksi, sources=[((12, 14, 10), sig)],
+              receivers=[tuple(int(v) for v in rng.integers(5, 25, 3)) for _ in range(4)], steps=600)
+    r64, _ = oracle.simulate(precision="f64", **kw)
+    r32, _ = oracle.simulate(precision="f32", **kw)
+    r16, _ = oracle.simulate(precision="f16", **kw)
+    db = lambda x: 20 * np.log10(np.linalg.norm(x - r64) / np.linalg.norm(r64))
+    assert db(r16.astype(np.float64)) <= -40.0
+    assert db(r32.astype(np.float64)) <= -80.0
+    assert not np.array_equal(r16, r32)

@@ -45,7 +45,7 @@ def test_end_of_input_ends_the_loop():
 
 def test_error_lines():
     rc, out, _ = session(["frobnicate", "load", "run abc", "load /no/such/file.xml", "sdt tpu",
-                          "minsize [1,x,3]", "pml 1.5", "addmic [1,2,3]", "", "quit"])
+                          "minsize [1,x,3]", "pml 1.5", "addmic [1,2,3]", "", "precision fp8", "quit"])
     r = replies(out)
     assert r[0] == "Error: unrecognized command"
     assert r[1] == "Error: command load takes 1 argument(s)"
@@ -56,6 +56,7 @@ def test_error_lines():
     assert r[6] == "Error: argument[0] should be a(n) int"
     assert r[7].startswith("Error: no active simulation")
     assert r[8] == ""  # empty line: prompt again
+    assert r[9] == "Valid command arguments are 'fp32' or 'fp16'"
 
 
 def test_cd_and_lsd_without_device():
