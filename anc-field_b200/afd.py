@@ -35,7 +35,7 @@ EXPORTS = [
     "afd_model_last_error", "afd_model_destroy", "afd_check_filters", "afd_check_filters_static",
     "afd_create", "afd_set_min_size", "afd_load", "afd_set_model", "afd_set_pml",
     "afd_set_pml_profile", "afd_add_source", "afd_add_source_cell", "afd_add_receiver",
-    "afd_add_receiver_cell", "afd_run", "afd_get_receivers", "afd_update_source",
+    "afd_add_receiver_cell", "afd_run", "afd_prepare", "afd_get_receivers", "afd_update_source",
     "afd_get_receivers_range", "afd_get_field", "afd_get_plane",
     "afd_get_info", "afd_energy", "afd_set_stream", "afd_kernel_stats", "afd_last_error",
     "afd_destroy",
@@ -108,6 +108,7 @@ def library(path=LIB_PATH):
         "afd_add_receiver": (C.c_int, [vp, P(f32)]),
         "afd_add_receiver_cell": (C.c_int, [vp, P(i32)]),
         "afd_run": (C.c_int, [vp, i64, PROGRESS_FN, vp]),
+        "afd_prepare": (C.c_int, [vp, i64]),
         "afd_get_receivers": (C.c_int, [vp, i32, P(f32), i64]),
         "afd_update_source": (C.c_int, [vp, i64, i64, P(f32), i64]),
         "afd_get_receivers_range": (C.c_int, [vp, i32, i64, i64, P(f32), i64]),
@@ -316,6 +317,11 @@ class Simulation:
             cb = PROGRESS_FN(_cb)
         self._cb = cb
         self._check(library().afd_run(self._h, int(steps), cb, None))
+
+    def prepare(self, steps):
+        """Setup work of Run(steps) (buffers, uploads, CUDA graphs) without
+        running a step."""
+        self._check(library().afd_prepare(self._h, int(steps)))
 
     def mics(self, batch=0):
         info = self.info()

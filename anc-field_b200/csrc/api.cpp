@@ -296,6 +296,10 @@ int afd_run(afd_sim* s, int64_t steps, afd_progress_fn cb, void* user) {
     return status;
 }
 
+int afd_prepare(afd_sim* s, int64_t steps) {
+    SIM_CALL(s, { s->eng->prepare(steps); });
+}
+
 int afd_get_receivers(afd_sim* s, int32_t batch, float* out, int64_t cap) {
     SIM_CALL(s, {
         if (!out && cap > 0) throw afd::Error(AFD_ERR_ARG, "null output");

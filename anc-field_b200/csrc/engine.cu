@@ -646,6 +646,17 @@ __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ Ste
     store4(P.fi[AX][lv] + base + i, out, m);
 }
 
+// Eight binary16 values (one 16-byte word) as FP32 numbers.
+__device__ __forceinline__ void cvt8(const uint4 w, float v[8]) {
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&ws[q]));
+        v[2 * q] = f.x;
+        v[2 * q + 1] = f.y;
+    }
+}
+
 // Interior SLF update of every cell 1..n-2 (leapfrog.cl:34-55) streamed
 // through shared memory; see fused.cuh. Consumer warps wait on the stage
 // barriers independently (no block-wide barrier), so a slow warp delays
@@ -702,7 +713,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                 }
                 slot[s0] = item;
                 const FusedItem it = fused_item(f, item, nz);
-                const int x0 = it.tx * FT_X, y0 = it.ty * FT_Y;
+                const int x0 = it.tx * TL::W, y0 = it.ty * FT_Y;
                 const int zc = (wc * B + it.b) * nz, zo = (wo * B + it.b) * nz;
                 for (int z = it.z0 - 1; z <= it.z1; ++z, ++k) {
                     const int s = (int)(k % F_STAGES);
@@ -728,7 +739,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
     }
 
     const int lane = tid & 31;
-    const int cx = (tid & 15) * 4, cy = tid >> 4;
+    const int cx = (tid & 15) * TL::CPT, cy = tid >> 4;
     const float L2 = a.lambda2, CI = a.cint;
     uint32_t k = 0;
     while (true) {
@@ -739,10 +750,10 @@ __global__ void __launch_bounds__(F_THREADS, 2)
         const int item = slot[k % F_STAGES];
         if (item < 0) break;
         const FusedItem it = fused_item(f, item, nz);
-        const int x = it.tx * FT_X + cx, y = it.ty * FT_Y + cy;
+        const int x = it.tx * TL::W + cx, y = it.ty * FT_Y + cy;
         T* pn = level_ptr<T>(a, wn) + (size_t)it.b * a.g.vol + (int64_t)y * a.g.pitch + x;
         const bool yok = (y >= 1 && y <= a.g.ny - 2);
-        const bool xfull = (x >= 1 && x + 3 <= a.g.nx - 2);
+        const bool xfull = (x >= 1 && x + TL::CPT - 1 <= a.g.nx - 2);
         const int planes = it.z1 - it.z0;
         if (!mbar_wait(&full[(k + 1) % F_STAGES], ((k + 1) / F_STAGES) & 1)) {
             if (lane == 0) atomicOr(a.flag, 2);
@@ -790,71 +801,118 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                 }
             }
         } else {
+            // FP16: 8 cells per thread. p^n of planes z-1 and z stays in
+            // registers from plane to plane: each plane loads and converts
+            // only z+1, y+-1 and p^{n-1}. The update runs on stored values
+            // of level g-1 (scale s_cur) and is rescaled once at the end.
             const StepScales sc = step_scales(a.f16, it.b, g);
-            const float rc = sc.s_new * sc.inv_cur, ro = sc.s_new * sc.inv_old;
-            // cells of this thread's row that are grid-interior: their |p^n|
-            // (binary16 magnitude bits order as the values) enter the maximum
-            const uint32_t mlo = (yok && x >= 1 && x <= a.g.nx - 2 ? 0x7fffu : 0u) |
-                                 (yok && x + 1 >= 1 && x + 1 <= a.g.nx - 2 ? 0x7fff0000u : 0u);
-            const uint32_t mhi = (yok && x + 2 >= 1 && x + 2 <= a.g.nx - 2 ? 0x7fffu : 0u) |
-                                 (yok && x + 3 >= 1 && x + 3 <= a.g.nx - 2 ? 0x7fff0000u : 0u);
-            uint32_t amax = 0;
-            for (int pl = 0; pl < planes; ++pl) {
+            const float rc = sc.s_new * sc.inv_cur, ro = sc.s_cur * sc.inv_old;
+            uint32_t vmask[4];
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const int x0c = x + 2 * w;
+                vmask[w] = (yok && x0c >= 1 && x0c <= a.g.nx - 2 ? 0x7fffu : 0u) |
+                           (yok && x0c + 1 >= 1 && x0c + 1 <= a.g.nx - 2 ? 0x7fff0000u : 0u);
+            }
+            const int s0 = (cy + 1) * TL::HX + cx + TL::XOFF;
+            const int so = cy * TL::W + cx;
+            float ra[8], rb[8], rcv[8];
+            uint4 wa, wb, wc;  // raw words of the rows in ra, rb, rcv
+            {
+                const __half* Pm = reinterpret_cast<const __half*>(smem + (k % F_STAGES) * TL::STAGE);
+                const __half* P0 = reinterpret_cast<const __half*>(smem + ((k + 1) % F_STAGES) * TL::STAGE);
+                wa = *reinterpret_cast<const uint4*>(Pm + s0);
+                wb = *reinterpret_cast<const uint4*>(P0 + s0);
+                cvt8(wa, ra);
+                cvt8(wb, rb);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[k % F_STAGES]);  // plane z0-1 now in registers
+            uint32_t amax = 0, omax = 0;
+            // one plane: zm, c, zp rotate through ra, rb, rcv
+            auto plane = [&](int pl, float (&zm)[8], float (&c)[8], float (&zp)[8], const uint4& cw,
+                             uint4& zpw) -> bool {
                 const int z = it.z0 + pl;
-                const uint32_t kc = k + 1 + pl, kp = kc + 1, km = kc - 1;
-                if (!mbar_wait(&full[kp % F_STAGES], (kp / F_STAGES) & 1)) {
-                    if (lane == 0) atomicOr(a.flag, 2);
-                    return;
-                }
+                const uint32_t kc = k + 1 + pl, kp = kc + 1;
+                if (!mbar_wait(&full[kp % F_STAGES], (kp / F_STAGES) & 1)) return false;
                 const __half* P0 = reinterpret_cast<const __half*>(smem + (kc % F_STAGES) * TL::STAGE);
-                const __half* Pm = reinterpret_cast<const __half*>(smem + (km % F_STAGES) * TL::STAGE);
                 const __half* Pp = reinterpret_cast<const __half*>(smem + (kp % F_STAGES) * TL::STAGE);
                 const __half* O =
                     reinterpret_cast<const __half*>(smem + (kc % F_STAGES) * TL::STAGE + TL::PN_PAD);
-                const int s0 = (cy + 1) * TL::HX + cx + TL::XOFF;
-                const uint2 cr = *reinterpret_cast<const uint2*>(P0 + s0);
-                const float xm = __half2float(P0[s0 - 1]), xp = __half2float(P0[s0 + 4]);
-                const uint2 ymr = *reinterpret_cast<const uint2*>(P0 + s0 - TL::HX);
-                const uint2 ypr = *reinterpret_cast<const uint2*>(P0 + s0 + TL::HX);
-                const uint2 zmr = *reinterpret_cast<const uint2*>(Pm + s0);
-                const uint2 zpr = *reinterpret_cast<const uint2*>(Pp + s0);
-                const uint2 orw = *reinterpret_cast<const uint2*>(O + cy * FT_X + cx);
+                const uint4 ymw = *reinterpret_cast<const uint4*>(P0 + s0 - TL::HX);
+                const uint4 ypw = *reinterpret_cast<const uint4*>(P0 + s0 + TL::HX);
+                zpw = *reinterpret_cast<const uint4*>(Pp + s0);
+                const uint4 ow = *reinterpret_cast<const uint4*>(O + so);
+                const float xm = __half2float(P0[s0 - 1]), xp = __half2float(P0[s0 + 8]);
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
-                amax = max(amax, max(max(cr.x & mlo & 0x7fffu, (cr.x & mlo) >> 16),
-                                     max(cr.y & mhi & 0x7fffu, (cr.y & mhi) >> 16)));
-                auto h2 = [](uint32_t w) { return __half22float2(*reinterpret_cast<const __half2*>(&w)); };
-                const float2 c01 = h2(cr.x), c23 = h2(cr.y);
-                const float2 ym01 = h2(ymr.x), ym23 = h2(ymr.y), yp01 = h2(ypr.x), yp23 = h2(ypr.y);
-                const float2 zm01 = h2(zmr.x), zm23 = h2(zmr.y), zp01 = h2(zpr.x), zp23 = h2(zpr.y);
-                const float2 o01 = h2(orw.x), o23 = h2(orw.y);
-                float4 v;
-                v.x = slf_update_scaled(L2, rc, ro, c01.y, xm, yp01.x, ym01.x, zp01.x, zm01.x, c01.x, o01.x);
-                v.y = slf_update_scaled(L2, rc, ro, c23.x, c01.x, yp01.y, ym01.y, zp01.y, zm01.y, c01.y, o01.y);
-                v.z = slf_update_scaled(L2, rc, ro, c23.y, c01.y, yp23.x, ym23.x, zp23.x, zm23.x, c23.x, o23.x);
-                v.w = slf_update_scaled(L2, rc, ro, xp, c23.x, yp23.y, ym23.y, zp23.y, zm23.y, c23.y, o23.y);
-                bad |= !(f16_finite(v.x) && f16_finite(v.y) && f16_finite(v.z) && f16_finite(v.w));
+                if (lane == 0) mbar_arrive(&empty[kc % F_STAGES]);  // plane z read
+                amax = __vmaxu2(amax, __vmaxu2(__vmaxu2(cw.x & vmask[0], cw.y & vmask[1]),
+                                               __vmaxu2(cw.z & vmask[2], cw.w & vmask[3])));
+                float ym[8], yp[8], o[8];
+                cvt8(ymw, ym);
+                cvt8(ypw, yp);
+                cvt8(zpw, zp);
+                cvt8(ow, o);
+                uint32_t outw[4];
+#pragma unroll
+                for (int w = 0; w < 4; ++w) {
+                    float v2[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int m = 2 * w + h;
+                        const float xl = m == 0 ? xm : c[m - 1];
+                        const float xr = m == 7 ? xp : c[m + 1];
+                        float s = xr + xl;
+                        s = s + yp[m];
+                        s = s + ym[m];
+                        s = s + zp[m];
+                        s = s + zm[m];
+                        v2[h] = (c[m] + ((c[m] - o[m] * ro) + L2 * (s - 6.0f * c[m]))) * rc;
+                    }
+                    const __half2 hv = __floats2half2_rn(v2[0], v2[1]);
+                    outw[w] = *reinterpret_cast<const uint32_t*>(&hv);
+                    omax = __vmaxu2(omax, outw[w] & 0x7fff7fffu);
+                }
                 if (yok) {
                     __half* dst = pn + (int64_t)z * a.g.plane;
                     if (xfull) {
-                        const __half2 lo = __floats2half2_rn(v.x, v.y), hi = __floats2half2_rn(v.z, v.w);
-                        uint2 w;
-                        w.x = *reinterpret_cast<const uint32_t*>(&lo);
-                        w.y = *reinterpret_cast<const uint32_t*>(&hi);
-                        __stcs(reinterpret_cast<uint2*>(dst), w);
+                        __stcs(reinterpret_cast<uint4*>(dst), make_uint4(outw[0], outw[1], outw[2], outw[3]));
                     } else {
-                        const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (x + m >= 1 && x + m <= a.g.nx - 2) dst[m] = __float2half_rn(vv[m]);
+                        for (int m = 0; m < 8; ++m)
+                            if (x + m >= 1 && x + m <= a.g.nx - 2)
+                                reinterpret_cast<unsigned short*>(dst)[m] =
+                                    (unsigned short)(outw[m >> 1] >> (16 * (m & 1)));
                     }
                 }
+                return true;
+            };
+            bool ok = true;
+            for (int pl = 0; pl < planes && ok; pl += 3) {
+                ok = plane(pl, ra, rb, rcv, wb, wc);
+                if (ok && pl + 1 < planes) ok = plane(pl + 1, rb, rcv, ra, wc, wa);
+                if (ok && pl + 2 < planes) ok = plane(pl + 2, rcv, ra, rb, wa, wb);
             }
-            const uint32_t wmax = __reduce_max_sync(0xffffffffu, amax);
-            if (lane == 0 && wmax) {
-                const float m = __half2float(__ushort_as_half((unsigned short)wmax)) * sc.inv_cur;
-                atomicMax(a.f16.mx + (size_t)it.b * 5 + max_slot(g - 1), __float_as_uint(m));
+            if (!ok) {
+                if (lane == 0) atomicOr(a.flag, 2);
+                return;
             }
+            // the plane z1 loaded last is the next item's halo: release it
+            // together with the others below
+            const uint32_t gmax = __reduce_max_sync(0xffffffffu, max(amax & 0xffffu, amax >> 16));
+            if (lane == 0 && gmax) {
+                const float mv = __half2float(__ushort_as_half((unsigned short)gmax)) * sc.inv_cur;
+                atomicMax(a.f16.mx + (size_t)it.b * 5 + max_slot(g - 1), __float_as_uint(mv));
+            }
+            // a stored binary16 infinity or NaN (magnitude bits >= 0x7c00)
+            // in a grid-interior cell means the field left the range
+            const uint32_t om = max(omax & 0xffffu, omax >> 16);
+            bad = om >= 0x7c00u;
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[(k + planes + 1) % F_STAGES]);
+            if (__any_sync(0xffffffffu, bad && yok && x <= a.g.nx - 2) && lane == 0) atomicOr(a.flag, 1);
+            k += (uint32_t)planes + 2;
+            continue;
         }
         __syncwarp();
         if (lane == 0) {
@@ -1126,6 +1184,7 @@ struct Engine::Impl {
     void launch_step_count_only(int64_t n) { launches += kernels_per_step() * n + 1; }
     cudaGraphExec_t graph_for(int64_t n);
     void run_chunk(int64_t n);
+    void setup_run(int64_t steps);
     void collect_profile();
 };
 
@@ -1152,7 +1211,8 @@ void Engine::Impl::init_device() {
         if (!f16_smax.ptr) f16_smax.alloc((size_t)prm.batch);
     }
 
-    tiles_x = (nx + FT_X - 1) / FT_X;
+    const int tile_w = f16() ? Tile<__half>::W : Tile<float>::W;
+    tiles_x = (nx + tile_w - 1) / tile_w;
     tiles_y = (ny + FT_Y - 1) / FT_Y;
     // boundary list, sorted by (tile, plane, position in tile) for the fused
     // kernel; the unfused kernel takes any order
@@ -1206,7 +1266,7 @@ void Engine::Impl::init_device() {
         const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)(3 * prm.batch * nz)};
         const cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)plane * es};
         const cuuint32_t box_h[3] = {(cuuint32_t)(f16() ? Tile<__half>::HX : Tile<float>::HX), FH_Y, 1},
-                         box_o[3] = {FT_X, FT_Y, 1}, estr[3] = {1, 1, 1};
+                         box_o[3] = {(cuuint32_t)tile_w, FT_Y, 1}, estr[3] = {1, 1, 1};
         CUresult r1 = enc(&tm_halo, dt, 3, fields.ptr, dims, strides, box_h, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -1879,25 +1939,50 @@ void Engine::add_receiver_pos(const float pos[3]) {
 // reports progress (step 0 and every 200th step), so a chunk is one
 // captured graph replay; the REF-mode PML fields are zeroed after every
 // 8000th step of the run (simulation.hpp:411-430).
+// Device state for a run of `steps` more steps: model, PML, sources,
+// receiver record, streaming plan and kernel arguments.
+void Engine::Impl::setup_run(int64_t steps) {
+    if (steps < 0) throw Error(AFD_ERR_ARG, "steps must be >= 0");
+    CK(cudaSetDevice(device));
+    if (!initialized) init_device();
+    if (pml_dirty) {
+        setup_pml();
+        drop_graphs();
+    }
+    if (src_dirty) {
+        upload_sources();
+        drop_graphs();
+    }
+    ensure_receivers(steps_done + steps);
+    if (use_fused() && fused_dirty) {
+        build_fused();
+        drop_graphs();
+    }
+    build_args();
+}
+
+// Chunks of a run: step 0 alone, then up to 200 steps (the progress
+// points of simulation.hpp:403-409).
+static std::vector<int64_t> run_chunks(int64_t steps) {
+    std::vector<int64_t> out;
+    for (int64_t i = 0; i < steps;) {
+        const int64_t n = (i == 0) ? 1 : std::min<int64_t>(200, steps - i);
+        out.push_back(n);
+        i += n;
+    }
+    return out;
+}
+
+void Engine::prepare(int64_t steps) {
+    Impl& D = *d_;
+    D.setup_run(steps);
+    if (D.prm.graphs && !D.prm.profile)
+        for (int64_t n : run_chunks(steps)) D.graph_for(n);
+}
+
 int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     Impl& D = *d_;
-    if (steps < 0) throw Error(AFD_ERR_ARG, "steps must be >= 0");
-    CK(cudaSetDevice(D.device));
-    if (!D.initialized) D.init_device();
-    if (D.pml_dirty) {
-        D.setup_pml();
-        D.drop_graphs();
-    }
-    if (D.src_dirty) {
-        D.upload_sources();
-        D.drop_graphs();
-    }
-    D.ensure_receivers(D.steps_done + steps);
-    if (D.use_fused() && D.fused_dirty) {
-        D.build_fused();
-        D.drop_graphs();
-    }
-    D.build_args();
+    D.setup_run(steps);
     D.launches = 0;
     for (auto& st : D.kstats) {
         st.launches = 0;

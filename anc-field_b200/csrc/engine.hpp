@@ -33,6 +33,7 @@ public:
     void add_receiver_cell(const int32_t ijk[3]);
     void add_receiver_pos(const float pos[3]);
     int run(int64_t steps, afd_progress_fn cb, void* user);
+    void prepare(int64_t steps);
     void get_receivers(int32_t batch, float* out, int64_t cap);
     void get_receivers_range(int32_t batch, int64_t t0, int64_t t1, float* out, int64_t cap);
     void update_source(int64_t index, int64_t t0, const float* sig, int64_t len);

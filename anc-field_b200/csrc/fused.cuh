@@ -35,24 +35,28 @@ constexpr int F_THREADS = F_CONSUMERS + 32;
 constexpr size_t F_SMEM = (size_t)F_STAGES * F_STAGE_BYTES + 2 * F_STAGES * 8 + F_STAGES * 4 + 128;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s
 
-// Stage layout per storage type. FP16 levels: the halo box starts 8 cells
-// before the tile (x times 2 bytes stays a multiple of 16) and is 80 cells
-// wide; 4.9 KB of each 5 KB stage is copied.
+// Stage layout per storage type. FP16 levels: 128-cell tiles (a stage
+// holds the same bytes as an FP32 one), the halo box starts 8 cells before
+// the tile (x times 2 bytes stays a multiple of 16) and is 144 cells wide.
 template <typename T>
 struct Tile;
+// W: tile width in cells; CPT: cells per consumer thread (16 threads per
+// row, 16 rows).
 template <>
 struct Tile<float> {
+    static constexpr int W = FT_X, CPT = 4;
     static constexpr int HX = FH_X, XOFF = 4, PN_PAD = F_PN_PAD, STAGE = F_STAGE_BYTES, TX = F_TX_BYTES;
     static constexpr size_t SMEM = F_SMEM;
 };
 template <>
 struct Tile<__half> {
-    static constexpr int HX = FT_X + 16, XOFF = 8;
-    static constexpr int PN_BYTES = HX * FH_Y * 2;                               // 2880
-    static constexpr int PN_PAD = (PN_BYTES + 127) / 128 * 128;                  // 2944
-    static constexpr int PO_BYTES = FT_X * FT_Y * 2;                             // 2048
-    static constexpr int STAGE = (PN_PAD + PO_BYTES + 127) / 128 * 128;          // 5120
-    static constexpr int TX = PN_BYTES + PO_BYTES;                               // 4928
+    static constexpr int W = 2 * FT_X, CPT = 8;
+    static constexpr int HX = W + 16, XOFF = 8;
+    static constexpr int PN_BYTES = HX * FH_Y * 2;                               // 5184
+    static constexpr int PN_PAD = (PN_BYTES + 127) / 128 * 128;                  // 5248
+    static constexpr int PO_BYTES = W * FT_Y * 2;                                // 4096
+    static constexpr int STAGE = (PN_PAD + PO_BYTES + 127) / 128 * 128;          // 9344
+    static constexpr int TX = PN_BYTES + PO_BYTES;                               // 9280
     static constexpr size_t SMEM = (size_t)F_STAGES * STAGE + 2 * F_STAGES * 8 + F_STAGES * 4 + 128;
 };
 
@@ -92,12 +96,17 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 // Bounded wait: false after kWaitLimitNs without the phase completing.
+// The clock is read once per 16 polls, so waiting warps issue few
+// instructions beside the ones that compute.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
-    while (!mbar_try(bar, parity))
+    for (;;) {
+#pragma unroll 1
+        for (int i = 0; i < 16; ++i)
+            if (mbar_try(bar, parity)) return true;
         if (global_ns() - t0 > kWaitLimitNs) return false;
-    return true;
+    }
 }
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
                                             uint64_t* bar) {

@@ -201,6 +201,12 @@ int afd_add_receiver_cell(afd_sim* s, const int32_t ijk[3]);
  * time steps; the time index continues across runs. */
 int afd_run(afd_sim* s, int64_t steps, afd_progress_fn cb, void* user);
 
+/* No counterpart in the reference: does the setup work of
+ * afd_run(s, steps, ...) without running a step (device buffers, uploads,
+ * the CUDA graphs of the run's chunks), so that a caller timing the run on
+ * the device measures only the steps. */
+int afd_prepare(afd_sim* s, int64_t steps);
+
 /* Receiver signals of one batch member, [n_receivers][t_end] row-major,
  * t_end = total steps run so far (the `save` layout, datafile.hpp:87-94). */
 int afd_get_receivers(afd_sim* s, int32_t batch, float* out, int64_t cap);
