@@ -238,3 +238,20 @@ def test_filter_check_host_path(pkg):
     a2[1] = -a2[1]                 # negative real part: not passive
     st, _, _ = pkg.check_filters(a2, b2)
     assert st[0] & 1 and st[1] & 2
+
+
+def test_library_exports_the_surrogate_entry_points(pkg):
+    """include/afd_surrogate.h: the surrogate network and its GEMM."""
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "afd_surrogate.h")).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(afd_[a-z0-9_]+)\s*\(", text)))
+    lib = pkg.afd.library()
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(pkg.surrogate.EXPORTS) == names
+
+
+def test_surrogate_rejects_untiled_sizes(pkg):
+    with pytest.raises(pkg.AfdError) as ei:
+        pkg.surrogate.Mlp(hidden=100)
+    assert ei.value.status == pkg.afd.ERR_ARG
+    assert "multiples of 128" in str(ei.value)
