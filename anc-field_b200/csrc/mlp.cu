@@ -9,7 +9,7 @@
 // both orientations for the GEMMs; activations and their gradients in BF16.
 //
 // GEMM: C[M][N] = A[M][K] * B[N][K]^T, both operands K-major BF16, one
-// 128 x 128 output tile per CTA, K in steps of 64 through a 4-stage TMA
+// 128 x 128 output tile per CTA, K in steps of 64 through a 3-stage TMA
 // ring. Warp 0 (one thread) streams tiles, warp 1 allocates TMEM and one
 // of its threads issues tcgen05.mma (K = 16 per instruction) and commits
 // stage releases, warps 2-5 read the accumulator with tcgen05.ld and run
@@ -46,7 +46,7 @@ struct Err : std::runtime_error {
         if (e__ != cudaSuccess) throw Err(AFD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
     } while (0)
 
-constexpr int TM = 128, TN = 128, TK = 64, NST = 4;
+constexpr int TM = 128, TN = 128, TK = 64, NST = 3;
 constexpr int A_BYTES = TM * TK * 2, B_BYTES = TN * TK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int GEMM_THREADS = 192;
 constexpr size_t GEMM_SMEM = 1024 + (size_t)NST * STAGE_BYTES + 256;
@@ -70,8 +70,10 @@ struct GemmOut {
     int* flag;  // bit 0: a wait expired
 };
 
+// Two CTAs per SM (99 KB of shared memory and 128 TMEM columns each): one
+// CTA's epilogue and set-up overlap the other's MMAs.
 template <int EPI>
-__global__ void __launch_bounds__(GEMM_THREADS, 1)
+__global__ void __launch_bounds__(GEMM_THREADS, 2)
     k_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const GemmOut g) {
     extern __shared__ unsigned char raw[];
     unsigned char* sm = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
@@ -734,8 +736,8 @@ int afd_mlp_set_weights(afd_mlp* m, int32_t layer, const float* w, const float* 
 int afd_gemm_bf16(const void* a, const void* b, float* c, int32_t M, int32_t N, int32_t K, void* stream) {
     try {
         set_smem_attr();
-        Dev<int> flag;
-        flag.alloc(1);
+        static Dev<int> flag;  // the wait-expired flag, kept for the process
+        if (!flag.p) flag.alloc(1);
         Gemm g = make_gemm(EPI_F32, (const bf16*)a, (const bf16*)b, M, N, K, flag.p);
         g.o.c32 = c;
         g.o.ldc = N;

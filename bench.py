@@ -41,6 +41,9 @@ def parse():
                     help="NX,NY,NZ: the same construction at another size (profiling captures)")
     ap.add_argument("--legs", default="device,e2e,roofline,cpu",
                     help="comma list of device,e2e,roofline,cpu")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: the single-source throughput line (default); c3: batched secondary-path IRs/s; "
+                         "c5: the learned surrogate against the FDTD")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="field storage: fp32, or fp16 levels with per-level power-of-two scales")
     return ap.parse_args()
@@ -166,11 +169,86 @@ def cpu_reference(cfg, steps, budget_s=25.0, precision="f32"):
                       % (nx, ny, zs, steps, os.cpu_count(), t)}
 
 
+def bench_c3(pkg, args):
+    """Secondary-path identification: 16 wall-adjacent unit-impulse sources
+    in a 256x192x160 room (16 receivers, 8192 steps). IRs/s = sources x
+    receivers / wall seconds of the run (launches included, setup and
+    graph instantiation excluded), for the plain single-source path (one
+    source, per-step launches, no graph), the batched FP32 path (all 16
+    sources as batch members, graph-replayed chunks) and the batched FP16
+    path."""
+    import torch
+    W = pkg.workloads
+    cfg = W.config_c3()
+    steps = cfg.steps
+
+    def run(batch, graphs, storage):
+        sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, batch=batch, graphs=graphs, storage=storage)
+        sim.SetModel(pkg.Model.from_voxels(cfg.vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
+        sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi)
+        for m in range(batch):
+            for cell, sig in cfg.batch_sources[m]:
+                sim.AddSourceCell(cell, sig, batch=m)
+        for r in cfg.receivers:
+            sim.AddMicCell(r)
+        sim.prepare(steps)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        sim.Run(steps)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t
+        out = sim.mics(batch=0)
+        sim.close()
+        return wall, out
+
+    n_rcv = len(cfg.receivers)
+    n_src = len(cfg.batch_sources)
+    clocks = Clocks(0)
+    clocks.start()
+    t_plain, y_plain = run(1, 0, 0)
+    t_b32, y_b32 = run(n_src, 1, 0)
+    t_b16, y_b16 = run(n_src, 1, 1)
+    clk = clocks.stop()
+    v = n_src * n_rcv / t_b32
+    nx, ny, nz = cfg.dims
+    return {"metric": "secondary-path IRs/s", "value": v, "unit": "IRs/s", "n_gpus": 1, "steps": steps,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "%dx%dx%d room (C1 construction, PML z+), %d wall-adjacent unit-impulse sources "
+                                   "as batch members, %d receivers, %d steps" % (nx, ny, nz, n_src, n_rcv, steps),
+                       "ir_error": "batched member 0 equals the single-source run bit for bit: %s"
+                                   % bool(np.array_equal(y_plain, y_b32))},
+            "paths": {"plain_single_source_fp32": {"irs_per_s": n_rcv / t_plain, "run_s": t_plain},
+                      "batched_fp32": {"irs_per_s": v, "run_s": t_b32},
+                      "batched_fp16": {"irs_per_s": n_src * n_rcv / t_b16, "run_s": t_b16,
+                                       "member0_rel_l2_vs_fp32": float(np.linalg.norm(y_b16 - y_b32) /
+                                                                       np.linalg.norm(y_b32))}},
+            "clocks": clk}
+
+
+def bench_c5(pkg, args):
+    """The learned surrogate against the FDTD (see surrogate_workflow.run_c5)."""
+    import ancfield_b200.surrogate_workflow as SW
+    r = SW.run_c5(pkg)
+    r["fit"]["loss_curve"] = r["fit"]["loss_curve"][::4]
+    return {"metric": "secondary-path IRs/s", "value": r["irs_per_s"]["surrogate_with_fallback"], "unit": "IRs/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16", "data": "synthetic (FDTD-generated IRs)",
+            "config": {"workload": "surrogate: %d training pairs, %d held-out pairs, 1%% L2 fallback bound"
+                                   % (r["train_pairs"], r["held_out_pairs"])},
+            "surrogate": r}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     import __graft_entry__ as ge
     pkg = ge.load()
+    if args.workload != "c2" and args.impl == "b200":
+        if rank == 0:
+            line = bench_c3(pkg, args) if args.workload == "c3" else bench_c5(pkg, args)
+            print(json.dumps(line), flush=True)
+        return
     W = pkg.workloads
     legs = set(args.legs.split(","))
     dims = tuple(int(v) for v in args.grid.split(",")) if args.grid else (512, 384, 320)
