@@ -36,7 +36,7 @@ EXPORTS = [
     "afd_create", "afd_set_min_size", "afd_load", "afd_set_model", "afd_set_pml",
     "afd_set_pml_profile", "afd_add_source", "afd_add_source_cell", "afd_add_receiver",
     "afd_add_receiver_cell", "afd_run", "afd_prepare", "afd_get_receivers", "afd_update_source",
-    "afd_get_receivers_range", "afd_get_field", "afd_get_plane",
+    "afd_get_receivers_range", "afd_get_field", "afd_get_plane", "afd_set_capture", "afd_get_frames",
     "afd_get_info", "afd_energy", "afd_set_stream", "afd_kernel_stats", "afd_last_error",
     "afd_destroy",
 ]
@@ -114,6 +114,8 @@ def library(path=LIB_PATH):
         "afd_get_receivers_range": (C.c_int, [vp, i32, i64, i64, P(f32), i64]),
         "afd_get_field": (C.c_int, [vp, i32, P(f32), i64]),
         "afd_get_plane": (C.c_int, [vp, i32, i32, i32, P(f32), i64]),
+        "afd_set_capture": (C.c_int, [vp, i32, i32, i32, i32, i32]),
+        "afd_get_frames": (C.c_int, [vp, P(f32), i64, P(i64), i64, P(i32)]),
         "afd_get_info": (C.c_int, [vp, P(Info)]),
         "afd_energy": (C.c_int, [vp, i32, P(f64)]),
         "afd_set_stream": (C.c_int, [vp, vp]),
@@ -358,6 +360,24 @@ class Simulation:
         out = np.empty(shape, np.float32)
         self._check(library().afd_get_plane(self._h, batch, axis, index, _ptr(out, C.c_float), out.size))
         return out
+
+    def set_capture(self, axis, index, every, max_frames=64, batch=0):
+        """From the next Run on, copy a plane (the plane() layout) after every
+        `every`-th step of each run into a ring of max_frames device frames."""
+        self._check(library().afd_set_capture(self._h, batch, axis, index, every, max_frames))
+        self._cap = (axis, max_frames)
+
+    def frames(self):
+        """(frames [n, rows, cols], global step of each frame), oldest first."""
+        axis, mx = getattr(self, "_cap", (1, 0))
+        i = self.info()
+        shape = {0: (i.nz, i.ny), 1: (i.nz, i.nx), 2: (i.ny, i.nx)}[axis]
+        out = np.empty((mx,) + shape, np.float32)
+        steps = np.empty(max(mx, 1), np.int64)
+        n = C.c_int32()
+        self._check(library().afd_get_frames(self._h, _ptr(out, C.c_float), out.size, _ptr(steps, C.c_int64),
+                                             steps.size, C.byref(n)))
+        return out[:n.value], steps[:n.value]
 
     def energy(self, batch=0):
         e = C.c_double()

@@ -24,7 +24,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--expt-relaxed-c
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-I" + INC] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" + INC]
 
-CU_SOURCES = ["engine.cu", "filters.cu", "mlp.cu"]
+CU_SOURCES = ["engine.cu", "filters.cu", "mlp.cu", "lms.cu"]
 CXX_SOURCES = ["model.cpp", "api.cpp"]
 HEADERS = ["device.cuh", "engine.hpp", "model.hpp", "filters.hpp", "fused.cuh", "tc.cuh"]
 
@@ -59,7 +59,7 @@ def build(force=False, verbose=False):
     """Compiles every CUDA and C++ source; returns the library path."""
     for d in (OBJ, LIB, BIN):
         os.makedirs(d, exist_ok=True)
-    hdrs = [os.path.join(SRC, h) for h in HEADERS] + [os.path.join(INC, "afd.h"), os.path.join(INC, "afd_surrogate.h")]
+    hdrs = [os.path.join(SRC, h) for h in HEADERS] + [os.path.join(INC, "afd.h"), os.path.join(INC, "afd_surrogate.h"), os.path.join(INC, "afd_lms.h")]
     objs = []
     nvcc = _nvcc()
     for s in CU_SOURCES:

@@ -296,6 +296,17 @@ int afd_run(afd_sim* s, int64_t steps, afd_progress_fn cb, void* user) {
     return status;
 }
 
+int afd_set_capture(afd_sim* s, int32_t batch, int32_t axis, int32_t index, int32_t every, int32_t max_frames) {
+    SIM_CALL(s, { s->eng->set_capture(batch, axis, index, every, max_frames); });
+}
+
+int afd_get_frames(afd_sim* s, float* out, int64_t cap, int64_t* steps, int64_t steps_cap, int32_t* n_frames) {
+    SIM_CALL(s, {
+        const int32_t n = s->eng->get_frames(out, cap, steps, steps_cap);
+        if (n_frames) *n_frames = n;
+    });
+}
+
 int afd_prepare(afd_sim* s, int64_t steps) {
     SIM_CALL(s, { s->eng->prepare(steps); });
 }

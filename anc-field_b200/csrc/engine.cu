@@ -997,6 +997,40 @@ __global__ void k_src_rcv_inline(const __grid_constant__ StepArgs a, const __gri
     }
 }
 
+// Headless visualisation: copy_plane.cl:29-34 (the y plane of the newest
+// level, copied after every third step of a run by simulation.hpp:393-400)
+// for any axis, into a device ring of frames. Runs after the step's source
+// and receiver updates; copies when the run-local step index is a multiple
+// of `every` (decided on the device, so one graph serves every chunk).
+struct CaptureDev {
+    int32_t batch, axis, index, every, max_frames, rows, cols;
+    float* frames;             // [max_frames][rows][cols]
+    long long* frame_step;     // [max_frames] global step of each frame
+    const long long* run0;     // [0] global step at the start of the run, [1] frames captured before it
+};
+
+template <typename T>
+__global__ void k_capture(const __grid_constant__ StepArgs a, const CaptureDev c, int j) {
+    const long long g = *a.d_step + j;
+    const long long i = g - c.run0[0];
+    if (i % c.every) return;
+    const long long n = c.run0[1] + i / c.every;
+    const int slot = (int)(n % c.max_frames);
+    const float2 sc = new_level_scale<T>(a, c.batch, g);
+    const T* p = level_ptr<T>(a, buf_new(g)) + (size_t)c.batch * a.g.vol;
+    float* out = c.frames + (size_t)slot * c.rows * c.cols;
+    const int total = c.rows * c.cols;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int r = e / c.cols, q = e % c.cols;
+        int64_t idx;
+        if (c.axis == 0) idx = (int64_t)r * a.g.plane + (int64_t)q * a.g.pitch + c.index;        // [nz][ny] at x
+        else if (c.axis == 1) idx = (int64_t)r * a.g.plane + (int64_t)c.index * a.g.pitch + q;   // [nz][nx] at y
+        else idx = (int64_t)c.index * a.g.plane + (int64_t)r * a.g.pitch + q;                    // [ny][nx] at z
+        out[e] = fld(p + idx, sc.y);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) c.frame_step[slot] = g;
+}
+
 __global__ void k_advance(long long* d_step, int n) { *d_step += n; }
 
 // Discrete SLF energy between the two latest levels u1 (newest) and u0,
@@ -1112,6 +1146,22 @@ struct Engine::Impl {
     int64_t rcv_cap = 0;
     int32_t rcv_n_dev = 0;
     DBuf<long long> d_step;
+    // headless visualisation (afd_set_capture)
+    int32_t cap_batch = 0, cap_axis = 1, cap_index = 0, cap_every = 0, cap_max = 0;
+    bool cap_dirty = false;
+    int64_t cap_total = 0;  // frames captured so far
+    DBuf<float> cap_frames;
+    DBuf<long long> cap_steps, cap_run0;
+    CaptureDev cap{};
+    void advance_done(int64_t n) {
+        if (cap_every > 0 && n > 0) cap_total += (n + cap_every - 1) / cap_every;
+        steps_done += n;
+    }
+    void plane_dims(int32_t axis, int64_t* rows, int64_t* cols) const {
+        if (axis == 0) { *rows = nz; *cols = ny; }
+        else if (axis == 1) { *rows = nz; *cols = nx; }
+        else { *rows = ny; *cols = nx; }
+    }
     DBuf<int> d_flag;
     DBuf<double> d_energy;
 
@@ -1704,6 +1754,11 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         end();
         ++launches;
     }
+    if (cap_every > 0) {
+        const int total = cap.rows * cap.cols;
+        k_capture<T><<<(unsigned)std::min(592, (total + 255) / 256), 256, 0, stream>>>(a, cap, j);
+        ++launches;
+    }
 }
 
 cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
@@ -1766,6 +1821,7 @@ int64_t Engine::Impl::kernels_per_step() const {
                  (int64_t)pml_axis_boxes[2].size();
     }
     if (a.src.n > 0 || a.rcv.n > 0) ++k;
+    if (cap_every > 0) ++k;
     return k;
 }
 
@@ -1958,6 +2014,29 @@ void Engine::Impl::setup_run(int64_t steps) {
         build_fused();
         drop_graphs();
     }
+    if (cap_dirty) {
+        if (cap_every > 0) {
+            const int32_t dims[3] = {nx, ny, nz};
+            if (cap_batch < 0 || cap_batch >= prm.batch || cap_axis < 0 || cap_axis > 2 || cap_index < 0 ||
+                cap_index >= dims[cap_axis])
+                throw Error(AFD_ERR_ARG, "capture plane outside the grid");
+            int64_t rows, cols;
+            plane_dims(cap_axis, &rows, &cols);
+            cap_frames.alloc((size_t)cap_max * rows * cols);
+            cap_steps.alloc((size_t)cap_max);
+            if (!cap_run0.ptr) cap_run0.alloc(2);
+            cap = CaptureDev{cap_batch, cap_axis, cap_index, cap_every, cap_max, (int32_t)rows, (int32_t)cols,
+                             cap_frames.ptr, cap_steps.ptr, cap_run0.ptr};
+        }
+        cap_total = 0;
+        cap_dirty = false;
+        drop_graphs();
+    }
+    if (cap_every > 0) {
+        const long long r0[2] = {(long long)steps_done, (long long)cap_total};
+        CK(cudaMemcpyAsync(cap_run0.ptr, r0, sizeof(r0), cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
     build_args();
 }
 
@@ -2010,11 +2089,11 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
             int flag = 0;
             CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
             if (flag & 2) {
-                D.steps_done += i;
+                D.advance_done(i);
                 throw Error(AFD_ERR_CUDA, "step kernel pipeline wait timed out");
             }
             if (flag && D.prm.watchdog) {
-                D.steps_done += i;
+                D.advance_done(i);
                 throw Error(AFD_ERR_NUMERIC, std::string(D.f16() ? "pressure left the FP16 storage range"
                                                                  : "pressure left the finite bound |p| < 1e30") +
                                                  " by step " + std::to_string(D.steps_done));
@@ -2034,7 +2113,7 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     CK(cudaGetLastError());
     int flag = 0;
     CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-    D.steps_done += i;
+    D.advance_done(i);
     if (flag & 2) throw Error(AFD_ERR_CUDA, "step kernel pipeline wait timed out");
     if (flag && D.prm.watchdog)
         throw Error(AFD_ERR_NUMERIC, std::string(D.f16() ? "pressure left the FP16 storage range"
@@ -2149,6 +2228,39 @@ void Engine::get_field(int32_t batch, float* out, int64_t cap) {
     }
     CK(cudaMemcpy2D(out, D.nx * sizeof(float), f, D.pitch * sizeof(float), D.nx * sizeof(float),
                     (size_t)D.ny * D.nz, cudaMemcpyDeviceToHost));
+}
+
+void Engine::set_capture(int32_t batch, int32_t axis, int32_t index, int32_t every, int32_t max_frames) {
+    Impl& D = *d_;
+    if (every > 0 && (max_frames < 1 || max_frames > 1 << 20)) throw Error(AFD_ERR_ARG, "max_frames must be in 1..2^20");
+    if (axis < 0 || axis > 2) throw Error(AFD_ERR_ARG, "axis must be 0, 1 or 2");
+    D.cap_batch = batch;
+    D.cap_axis = axis;
+    D.cap_index = index;
+    D.cap_every = every > 0 ? every : 0;
+    D.cap_max = every > 0 ? max_frames : 0;
+    D.cap_dirty = true;
+}
+
+int32_t Engine::get_frames(float* out, int64_t cap, int64_t* steps, int64_t steps_cap) {
+    Impl& D = *d_;
+    if (D.cap_every <= 0 || !D.cap_frames.ptr || D.cap_dirty) return 0;
+    const int64_t n = std::min<int64_t>(D.cap_total, D.cap_max);
+    const int64_t fsz = (int64_t)D.cap.rows * D.cap.cols;
+    if (out && cap < n * fsz) throw Error(AFD_ERR_ARG, "output buffer too small: need " + std::to_string(n * fsz));
+    if (steps && steps_cap < n) throw Error(AFD_ERR_ARG, "steps buffer too small");
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamSynchronize(D.stream));
+    std::vector<long long> st((size_t)D.cap_max);
+    CK(cudaMemcpy(st.data(), D.cap_steps.ptr, st.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t slot = (D.cap_total - n + k) % D.cap_max;  // oldest first
+        if (out)
+            CK(cudaMemcpy(out + k * fsz, D.cap_frames.ptr + slot * fsz, (size_t)fsz * sizeof(float),
+                          cudaMemcpyDeviceToHost));
+        if (steps) steps[k] = st[(size_t)slot];
+    }
+    return (int32_t)n;
 }
 
 void Engine::get_plane(int32_t batch, int32_t axis, int32_t index, float* out, int64_t cap) {

@@ -8,8 +8,10 @@
 // the next simulation): `mode ref|fixed`, `dx <m>`, `c <m/s>`, `dt <s>`,
 // `fs <Hz>`, `pmlfaces <mask>`, `graphs 0|1`, `precision fp32|fp16` (FP16
 // field storage, with `mode fixed`). `vis` is headless: it records
-// the y level; `visdump <file>` writes that plane of the latest field as
-// text rows.
+// the y level and captures that plane on the device after every third step
+// of a run (as the reference feeds its MJPEG stream); `visdump <file>`
+// writes the plane of the latest field as text rows, or, for a file name
+// ending in .npy, every captured frame as a float32 [frames][nz][nx] array.
 #include <unistd.h>
 
 #include <cerrno>
@@ -225,7 +227,11 @@ struct Repl {
             float level;
             parse_float(a[0], &level);
             vis_level = (int)(level / prm.dx);
-            std::cerr << "vis: headless, plane y=" << vis_level << " kept on the device\n";
+            // simulation.hpp:393-400 copies this plane after every third step
+            // of a run; here into a ring of 64 device frames
+            int st = afd_set_capture(sim, 0, 1, vis_level, 3, 64);
+            if (st != AFD_OK) return fail_status(st);
+            std::cerr << "vis: headless, plane y=" << vis_level << " captured every 3 steps on the device\n";
         });
         add("visdump", {"string"}, [this](const std::vector<std::string>& a) {
             if (!need_sim()) return;
@@ -235,6 +241,16 @@ struct Repl {
             }
             afd_info info;
             afd_get_info(sim, &info);
+            const std::string& path = a[0];
+            if (path.size() > 4 && path.compare(path.size() - 4, 4, ".npy") == 0) {
+                // every captured frame, oldest first: float32 [frames][nz][nx]
+                std::vector<float> frames((size_t)64 * info.nx * info.nz);
+                int32_t n = 0;
+                int st = afd_get_frames(sim, frames.data(), (int64_t)frames.size(), nullptr, 0, &n);
+                if (st != AFD_OK) return fail_status(st);
+                if (!write_npy(path, frames.data(), n, info.nz, info.nx)) std::cout << "Error: cannot write " << path << "\n";
+                return;
+            }
             std::vector<float> plane((size_t)info.nx * info.nz);
             int st = afd_get_plane(sim, 0, 1, vis_level, plane.data(), (int64_t)plane.size());
             if (st != AFD_OK) return fail_status(st);
@@ -346,6 +362,24 @@ struct Repl {
             parse_int(a[0], &v);
             pml_faces = (uint32_t)v & 63u;
         });
+    }
+
+    // NumPy .npy (format 1.0) of a float32 [n][rows][cols] array.
+    static bool write_npy(const std::string& path, const float* data, int64_t n, int64_t rows, int64_t cols) {
+        std::string hdr = "{'descr': '<f4', 'fortran_order': False, 'shape': (" + std::to_string(n) + ", " +
+                          std::to_string(rows) + ", " + std::to_string(cols) + "), }";
+        while ((10 + hdr.size() + 1) % 64) hdr += ' ';
+        hdr += '\n';
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) return false;
+        const unsigned char magic[8] = {0x93, 'N', 'U', 'M', 'P', 'Y', 1, 0};
+        const uint16_t len = (uint16_t)hdr.size();
+        const unsigned char lenb[2] = {(unsigned char)(len & 0xff), (unsigned char)(len >> 8)};
+        bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(lenb, 1, 2, f) == 2 &&
+                  std::fwrite(hdr.data(), 1, hdr.size(), f) == hdr.size() &&
+                  std::fwrite(data, sizeof(float), (size_t)(n * rows * cols), f) == (size_t)(n * rows * cols);
+        ok = (std::fclose(f) == 0) && ok;
+        return ok;
     }
 
     static int progress(int64_t i, int64_t steps, void*) {

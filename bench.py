@@ -41,9 +41,10 @@ def parse():
                     help="NX,NY,NZ: the same construction at another size (profiling captures)")
     ap.add_argument("--legs", default="device,e2e,roofline,cpu",
                     help="comma list of device,e2e,roofline,cpu")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "lms", "gemm"],
                     help="c2: the single-source throughput line (default); c3: batched secondary-path IRs/s; "
-                         "c5: the learned surrogate against the FDTD")
+                         "c5: the learned surrogate against the FDTD; lms: LMS impulse-response estimation "
+                         "at the ie224-noise size; gemm: the surrogate's tcgen05 GEMM")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="field storage: fp32, or fp16 levels with per-level power-of-two scales")
     return ap.parse_args()
@@ -226,6 +227,81 @@ def bench_c3(pkg, args):
             "clocks": clk}
 
 
+def bench_lms(pkg, args):
+    """EstimateIr (anc_field_py/ancutil.py:24-37) at the size of
+    examples/ie224-noise.py: 64000 taps, 10 s at 32 kHz (320000 samples), 16
+    passes, mu 1e-4; synthetic band-limited noise through a decaying random
+    64000-tap response. Metric: LMS sample updates per second (samples x
+    passes / s). CPU baseline: the reference's loop (the bit-exact numpy
+    restatement) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lms_oracle
+    W = pkg.workloads
+    N, steps, epochs, mu = 64000, 320000, 16, 1e-4
+    rng = np.random.default_rng(21)
+    x = 0.1 * W.band_noise(steps, 32000.0, seed=22).astype(np.float64)  # mu N var(x) = 0.064 < 1: stable
+    h = rng.standard_normal(N) * np.exp(-np.arange(N) / 6000.0) * 0.05
+    d = np.fft.irfft(np.fft.rfft(x, 2 * steps) * np.fft.rfft(h, 2 * steps), 2 * steps)[:steps]
+    pkg.lms.estimate_ir(x[:4096], d[:4096], N, mu, epochs=1)  # warm-up
+    clocks = Clocks(0)
+    clocks.start()
+    t = time.perf_counter()
+    w = pkg.lms.estimate_ir(x, d, N, mu, epochs=epochs)
+    wall = time.perf_counter() - t
+    clk = clocks.stop()
+    value = steps * epochs / wall
+    # reference loop on a bounded sample: one pass over 3000 samples
+    ns = 3000
+    t = time.perf_counter()
+    lms_oracle.estimate(x[:ns], d[:ns], N, mu, epochs=1)
+    t_cpu = time.perf_counter() - t
+    return {"metric": "LMS sample updates/s", "value": value, "unit": "samples/s", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "LMS impulse-response estimation, %d taps, %d samples, %d passes, mu %g "
+                                   "(examples/ie224-noise.py size)" % (N, steps, epochs, mu),
+                       "run_s": wall, "w_rel_l2_vs_true_response": float(np.linalg.norm(w - h) / np.linalg.norm(h))},
+            "cpu_baseline": {"value": ns / t_cpu, "unit": "samples/s", "cores": 1, "kind": "port",
+                             "sample": "the reference's sample-serial loop (numpy, bit-exact restatement), "
+                                       "one pass over %d samples, %.1f s" % (ns, t_cpu)},
+            "clocks": clk}
+
+
+def bench_gemm(pkg, args):
+    """The surrogate's tcgen05 BF16 GEMM (FP32 accumulation) on 8192 x 4096
+    x 4096, device-timed with CUDA events, against the measured bf16 peak."""
+    import torch
+    M, N, K = 8192, 4096, 4096
+    a = torch.randn(M, K, device="cuda").to(torch.bfloat16)
+    b = torch.randn(N, K, device="cuda").to(torch.bfloat16)
+    c = torch.empty(M, N, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        pkg.surrogate.gemm_bf16(a, b, c, st)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record()
+    for _ in range(reps):
+        pkg.surrogate.gemm_bf16(a, b, c, st)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    tf = 2.0 * M * N * K / (ms / 1e3) / 1e12
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        src = "measured"
+    except Exception:
+        peak, src = 1590.0, "fallback"
+    err = float((c.double() - a.double() @ b.double().T).norm() / (a.double() @ b.double().T).norm())
+    return {"metric": "GEMM TFLOP/s", "value": tf, "unit": "TFLOP/s", "n_gpus": 1, "steps": reps, "warmup": 3,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic", "config": {"workload": "C = A B^T, %dx%dx%d, BF16 in, FP32 accumulate" % (M, N, K),
+                                            "rel_l2_vs_fp64": err},
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "peak_source": src, "unit": "TFLOP/s",
+                         "frac": tf / peak, "traffic": None}}
+
+
 def bench_c5(pkg, args):
     """The learned surrogate against the FDTD (see surrogate_workflow.run_c5)."""
     import ancfield_b200.surrogate_workflow as SW
@@ -246,7 +322,7 @@ def main():
     pkg = ge.load()
     if args.workload != "c2" and args.impl == "b200":
         if rank == 0:
-            line = bench_c3(pkg, args) if args.workload == "c3" else bench_c5(pkg, args)
+            line = {"c3": bench_c3, "c5": bench_c5, "lms": bench_lms, "gemm": bench_gemm}[args.workload](pkg, args)
             print(json.dumps(line), flush=True)
         return
     W = pkg.workloads

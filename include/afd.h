@@ -228,6 +228,20 @@ int afd_get_field(afd_sim* s, int32_t batch, float* out, int64_t cap);
 int afd_get_plane(afd_sim* s, int32_t batch, int32_t axis, int32_t index,
                   float* out, int64_t cap);
 
+/* Headless visualisation, replacing the copy of the newest level's y plane
+ * after every third step of a run for the MJPEG stream
+ * (simulation.hpp:393-400, copy_plane.cl:29-34): from the next run on, the
+ * plane of afd_get_plane(batch, axis, index) is copied on the device after
+ * every step whose index within the run is a multiple of `every`, into a
+ * ring of max_frames frames. every <= 0 turns it off. */
+int afd_set_capture(afd_sim* s, int32_t batch, int32_t axis, int32_t index, int32_t every,
+                    int32_t max_frames);
+/* The captured frames, oldest first: out[n][rows][cols] (the afd_get_plane
+ * layout), steps[n] the global step after which each was taken (either
+ * pointer may be NULL); *n_frames receives n <= max_frames. */
+int afd_get_frames(afd_sim* s, float* out, int64_t cap, int64_t* steps, int64_t steps_cap,
+                   int32_t* n_frames);
+
 typedef struct afd_info {
     int32_t nx, ny, nz;          /* simulation grid */
     int32_t ncoef, nmat;

@@ -101,7 +101,8 @@ def test_full_session_matches_oracle(pkg, tmp_path):
     mics = ["[0.7,0.5,0.4]", "[0.25,0.25,0.5]", "[0.9,0.1,0.1]"]
     lines = ["sdt gpu", "load %s" % (tmp_path / "model.xml"), "addsource [0.3,0.6,0.35] %s" % (tmp_path / "src.dat")]
     lines += ["addmic %s" % m for m in mics]
-    lines += ["run 0.0125", "save %s" % (tmp_path / "out.dat"), "quit"]
+    lines += ["vis 0.4", "run 0.0125", "save %s" % (tmp_path / "out.dat"), "visdump %s" % (tmp_path / "vis.npy"),
+              "quit"]
     rc, out, err = session(lines, timeout=300)
     assert rc == 0, err
     assert "added to active devices" in out
@@ -117,9 +118,15 @@ def test_full_session_matches_oracle(pkg, tmp_path):
     m = pkg.Model.load_kerkythea(str(tmp_path / "model.xml"), 0.02)
     a, b = m.coefs()
     cell = lambda p: tuple(int(np.float32(v) / np.float32(0.02)) for v in p)
-    want, _ = oracle.simulate(grid=m.dims[0], vox=m.voxels(), a=a, b=b, mode=0,
-                              sources=[(cell((0.3, 0.6, 0.35)), sig)],
-                              receivers=[cell(eval(s)) for s in mics], steps=400)
+    want, field = oracle.simulate(grid=m.dims[0], vox=m.voxels(), a=a, b=b, mode=0,
+                                  sources=[(cell((0.3, 0.6, 0.35)), sig)],
+                                  receivers=[cell(eval(s)) for s in mics], steps=400, want_field=True)
+    # vis 0.4: the plane y = 20 after every third step (134 of 400), the newest
+    # 64 kept on the device and dumped as .npy; the last is the final field's
+    frames = np.load(tmp_path / "vis.npy")
+    nx, ny, nz = m.dims[0]
+    assert frames.shape == (64, nz, nx) and frames.dtype == np.float32
+    assert np.array_equal(frames[-1], field[:, int(np.float32(0.4) / np.float32(0.02)), :])
     # the file holds ostream's 6 significant digits
     fmt = np.vectorize(lambda v: float("%.6g" % v))
     assert np.array_equal(got, fmt(want.astype(np.float64)))
