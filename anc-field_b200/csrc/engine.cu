@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -684,7 +685,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
     __syncthreads();
     const long long g = *a.d_step + j;
     const int B = a.batch, nz = a.g.nz;
-    const int n_items = f.tiles_x * f.tiles_y * f.n_chunks * B;
+    const int n_items = f.items ? f.n_items : f.tiles_x * f.tiles_y * f.n_chunks * B;
     const int wn = buf_new(g), wc = buf_cur(g), wo = buf_old(g);
 
     if (tid >= F_CONSUMERS) {
@@ -704,13 +705,14 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                     atomicOr(a.flag, 2);
                     break;
                 }
-                const int item = atomicAdd(f.work + j, 1);
-                if (item >= n_items) {
+                const int taken = atomicAdd(f.work + j, 1);
+                if (taken >= n_items) {
                     slot[s0] = -1;
                     mbar_arrive(&full[s0]);
                     ++k;
                     break;
                 }
+                const int item = f.items ? __ldg(f.items + taken) : taken;
                 slot[s0] = item;
                 const FusedItem it = fused_item(f, item, nz);
                 const int x0 = it.tx * TL::W, y0 = it.ty * FT_Y;
@@ -1169,6 +1171,7 @@ struct Engine::Impl {
     FusedDev fdev{};
     DBuf<int4> f_offs;
     DBuf<int> f_work;
+    DBuf<int> f_items;  // compact work list of the streaming kernel (FIXED scheme)
     CUtensorMap tm_halo{}, tm_own{};
     int fused_grid = 0;
     bool fused_dirty = true;
@@ -1228,6 +1231,33 @@ struct Engine::Impl {
     void ensure_receivers(int64_t t_end);
     void build_args();
     void launch_step(int j, bool profile);
+    // Runs independent launches concurrently: the first on `stream`, the
+    // others on side streams forked from it and joined back to it.
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> side_ev;
+    cudaEvent_t fork_ev = nullptr;
+    void run_side_by_side(const std::vector<std::function<void(cudaStream_t)>>& work) {
+        if (work.empty()) return;
+        const size_t extra = std::min<size_t>(work.size() - 1, 4);
+        while (side.size() < extra) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            side.push_back(s);
+            side_ev.push_back(e);
+        }
+        if (!fork_ev) CK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+        if (extra) {
+            CK(cudaEventRecord(fork_ev, stream));
+            for (size_t k = 0; k < extra; ++k) CK(cudaStreamWaitEvent(side[k], fork_ev, 0));
+        }
+        for (size_t w = 0; w < work.size(); ++w) work[w](w == 0 ? stream : side[(w - 1) % std::max<size_t>(extra, 1)]);
+        for (size_t k = 0; k < extra; ++k) {
+            CK(cudaEventRecord(side_ev[k], side[k]));
+            CK(cudaStreamWaitEvent(stream, side_ev[k], 0));
+        }
+    }
     template <typename T>
     void launch_step_t(int j, bool profile);
     int64_t kernels_per_step() const;
@@ -1353,7 +1383,47 @@ void Engine::Impl::build_fused() {
     F.n_chunks = (nz - 2 + dz - 1) / dz;
     if (!f_work.ptr) f_work.alloc(256);
     F.work = f_work.ptr;
-    fused_grid = (int)std::min<int64_t>(tiles * F.n_chunks, resident);
+    int64_t n_items = tiles * F.n_chunks;
+    // FIXED scheme: no air cell reads the value of a solid cell that is not
+    // within one cell of air, so items whose region widened by one cell on
+    // every side holds no air are left out (uneven rooms packed into one
+    // grid, thick walls). REF keeps every item: its X_M_Y_M_Z_M corner reads
+    // solid neighbours' leapfrog values.
+    f_items.release();
+    if (!ref() && have_model) {
+        const int W = f16() ? Tile<__half>::W : Tile<float>::W;
+        const int64_t ntile = (int64_t)tiles_x * tiles_y;
+        std::vector<uint8_t> flag((size_t)(ntile * nz), 0);  // [z][tile]: air within the widened footprint
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y) {
+                const int ty0 = std::max(0, (y - 1) / FT_Y), ty1 = std::min(tiles_y - 1, (y + 1) / FT_Y);
+                for (int x = 0; x < nx; ++x) {
+                    const bool air = x >= model.nx || y >= model.ny || z >= model.nz || model.at(x, y, z) == -1;
+                    if (!air) continue;
+                    const int tx0 = std::max(0, (x - 1) / W), tx1 = std::min(tiles_x - 1, (x + 1) / W);
+                    for (int ty = ty0; ty <= ty1; ++ty)
+                        for (int tx = tx0; tx <= tx1; ++tx) flag[(size_t)z * ntile + ty * tiles_x + tx] = 1;
+                }
+            }
+        std::vector<int> items;
+        for (int b = 0; b < prm.batch; ++b)
+            for (int c = 0; c < F.n_chunks; ++c) {
+                const int z0 = 1 + c * dz, z1 = std::min(z0 + dz, nz - 1);
+                for (int64_t t = 0; t < ntile; ++t) {
+                    bool need = false;
+                    for (int z = std::max(0, z0 - 1); z <= std::min(z1, nz - 1) && !need; ++z)
+                        need = flag[(size_t)z * ntile + t] != 0;
+                    if (need) items.push_back((int)((((int64_t)b * F.n_chunks + c) * tiles_y) * tiles_x + t));
+                }
+            }
+        if ((int64_t)items.size() < n_items) {
+            f_items.upload(items);
+            F.items = f_items.ptr;
+            F.n_items = (int32_t)items.size();
+            n_items = (int64_t)items.size();
+        }
+    }
+    fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));
     fused_dirty = false;
 }
 
@@ -1684,67 +1754,92 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         end();
         ++launches;
     }
-    if (a.lrs.n > 0) {
+    auto lrs_launch = [&](cudaStream_t st) {
         const dim3 grd((unsigned)((a.lrs.n + 255) / 256), (unsigned)prm.batch);
-        begin(KK_LRS);
         if constexpr (sizeof(T) == 4) {
-            if (ref()) launch_lrs<true, float>(a, j, grd, stream);
-            else launch_lrs<false, float>(a, j, grd, stream);
+            if (ref()) launch_lrs<true, float>(a, j, grd, st);
+            else launch_lrs<false, float>(a, j, grd, st);
         } else {
-            launch_lrs<false, T>(a, j, grd, stream);
+            launch_lrs<false, T>(a, j, grd, st);
         }
-        end();
         ++launches;
-    }
-    if (a.pml.width > 0) {
-        if (ref()) {
-            if (sizeof(T) == 4 && nx > 4 && ny > 4 && nz > 4) {
-                const dim3 grd((unsigned)((nx - 4 + 63) / 64), (unsigned)((ny - 4 + 3) / 4),
-                               (unsigned)((nz - 4) * prm.batch));
-                begin(KK_PML_AUX);
-                k_pml_ref_aux<<<grd, blk, 0, stream>>>(a, j);
-                end();
-                begin(KK_PML_P);
-                k_pml_ref_p<<<grd, blk, 0, stream>>>(a, j);
-                end();
-                launches += 2;
-            }
-        } else if (a.pml.n_units > 0) {
-            auto shape = [&](const PmlBox& bx, dim3& grd, dim3& blk) {
-                unsigned w = 1;
-                while ((int)w < bx.units && w < 32) w <<= 1;
-                blk = dim3(w, 256 / w, 1);
-                grd = dim3((unsigned)((bx.units + w - 1) / w), (unsigned)((bx.height + blk.y - 1) / blk.y),
-                           (unsigned)(bx.depth * prm.batch));
-            };
-            const bool psi = a.pml.psi_on != 0;
-            for (const PmlBox& bx : pml_boxes) {
-                dim3 grd, blk;
-                shape(bx, grd, blk);
-                begin(KK_PML_P);
-                if (psi) k_pml_box_p<true, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                else k_pml_box_p<false, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                end();
-                ++launches;
-            }
-            for (int ax = 0; ax < 3; ++ax)
-                for (const PmlBox& bx : pml_axis_boxes[ax]) {
-                    dim3 grd, blk;
-                    shape(bx, grd, blk);
+    };
+    auto shape = [&](const PmlBox& bx, dim3& grd, dim3& bk) {
+        unsigned w = 1;
+        while ((int)w < bx.units && w < 32) w <<= 1;
+        bk = dim3(w, 256 / w, 1);
+        grd = dim3((unsigned)((bx.units + w - 1) / w), (unsigned)((bx.height + bk.y - 1) / bk.y),
+                   (unsigned)(bx.depth * prm.batch));
+    };
+    const bool psi = a.pml.psi_on != 0;
+    auto pml_p_launch = [&](const PmlBox& bx, cudaStream_t st) {
+        dim3 grd, bk;
+        shape(bx, grd, bk);
+        if (psi) k_pml_box_p<true, T><<<grd, bk, 0, st>>>(a, bx, j);
+        else k_pml_box_p<false, T><<<grd, bk, 0, st>>>(a, bx, j);
+        ++launches;
+    };
+    auto pml_aux_launch = [&](int ax, const PmlBox& bx, cudaStream_t st) {
+        dim3 grd, bk;
+        shape(bx, grd, bk);
+        if (ax == 0) {
+            if (psi) k_pml_box_aux<0, true, T><<<grd, bk, 0, st>>>(a, bx, j);
+            else k_pml_box_aux<0, false, T><<<grd, bk, 0, st>>>(a, bx, j);
+        } else if (ax == 1) {
+            if (psi) k_pml_box_aux<1, true, T><<<grd, bk, 0, st>>>(a, bx, j);
+            else k_pml_box_aux<1, false, T><<<grd, bk, 0, st>>>(a, bx, j);
+        } else {
+            if (psi) k_pml_box_aux<2, true, T><<<grd, bk, 0, st>>>(a, bx, j);
+            else k_pml_box_aux<2, false, T><<<grd, bk, 0, st>>>(a, bx, j);
+        }
+        ++launches;
+    };
+    const bool fixed_pml = !ref() && a.pml.width > 0 && a.pml.n_units > 0;
+    if (fixed_pml && !profile && prm.graphs) {  // inside CUDA graphs: no host cost per step
+        // FIXED scheme: the boundary update and the PML pressure boxes write
+        // disjoint cells and read only levels n and n-1 and the old
+        // auxiliary fields, so they run side by side; the auxiliary updates
+        // (one per axis, disjoint outputs) follow once both are done.
+        std::vector<std::function<void(cudaStream_t)>> g1, g2;
+        if (a.lrs.n > 0) g1.push_back(lrs_launch);
+        for (const PmlBox& bx : pml_boxes) g1.push_back([&, bx](cudaStream_t st) { pml_p_launch(bx, st); });
+        for (int ax = 0; ax < 3; ++ax)
+            for (const PmlBox& bx : pml_axis_boxes[ax])
+                g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
+        run_side_by_side(g1);
+        run_side_by_side(g2);
+    } else {
+        if (a.lrs.n > 0) {
+            begin(KK_LRS);
+            lrs_launch(stream);
+            end();
+        }
+        if (a.pml.width > 0) {
+            if (ref()) {
+                if (sizeof(T) == 4 && nx > 4 && ny > 4 && nz > 4) {
+                    const dim3 grd((unsigned)((nx - 4 + 63) / 64), (unsigned)((ny - 4 + 3) / 4),
+                                   (unsigned)((nz - 4) * prm.batch));
                     begin(KK_PML_AUX);
-                    if (ax == 0) {
-                        if (psi) k_pml_box_aux<0, true, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                        else k_pml_box_aux<0, false, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                    } else if (ax == 1) {
-                        if (psi) k_pml_box_aux<1, true, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                        else k_pml_box_aux<1, false, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                    } else {
-                        if (psi) k_pml_box_aux<2, true, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                        else k_pml_box_aux<2, false, T><<<grd, blk, 0, stream>>>(a, bx, j);
-                    }
+                    k_pml_ref_aux<<<grd, blk, 0, stream>>>(a, j);
                     end();
-                    ++launches;
+                    begin(KK_PML_P);
+                    k_pml_ref_p<<<grd, blk, 0, stream>>>(a, j);
+                    end();
+                    launches += 2;
                 }
+            } else if (a.pml.n_units > 0) {
+                for (const PmlBox& bx : pml_boxes) {
+                    begin(KK_PML_P);
+                    pml_p_launch(bx, stream);
+                    end();
+                }
+                for (int ax = 0; ax < 3; ++ax)
+                    for (const PmlBox& bx : pml_axis_boxes[ax]) {
+                        begin(KK_PML_AUX);
+                        pml_aux_launch(ax, bx, stream);
+                        end();
+                    }
+            }
         }
     }
     if (a.src.n > 0 || a.rcv.n > 0) {
@@ -1866,6 +1961,9 @@ Engine::~Engine() {
     }
     if (D.ev0) cudaEventDestroy(D.ev0);
     if (D.ev1) cudaEventDestroy(D.ev1);
+    for (auto st : D.side) cudaStreamDestroy(st);
+    for (auto e : D.side_ev) cudaEventDestroy(e);
+    if (D.fork_ev) cudaEventDestroy(D.fork_ev);
     if (D.own_stream) cudaStreamDestroy(D.own_stream);
 }
 

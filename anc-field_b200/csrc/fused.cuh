@@ -63,7 +63,9 @@ struct Tile<__half> {
 // Work decomposition of the streaming kernel.
 struct FusedDev {
     int32_t tiles_x, tiles_y, dz, n_chunks;
-    int* work;  // work-item counters, one per launch of a chunk
+    int* work;          // work-item counters, one per launch of a chunk
+    const int* items;   // null: every item; else the n_items items to run (ascending)
+    int32_t n_items;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {

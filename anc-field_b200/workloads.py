@@ -278,3 +278,66 @@ def config_c3(steps=8192, seed=3, n_src=16, dims=(256, 192, 160)):
     cfg = Config("c3", (nx, ny, nz), vox, a, b, dx, c, dt, steps, [(srcs[0], imp)], rcv, 12, FACE_ZP, ksi,
                  mode=1, batch_sources=[[(s, imp)] for s in srcs])
     return cfg
+
+
+def pack_rooms(rooms, filler=0):
+    """Packs rooms of uneven size into one voxel grid so that one simulation
+    (one launch per kernel per step) advances them all. Each room is
+    int32 voxels [nz, ny, nx] with solid walls on every face except z+ (its
+    PML face). Rooms are placed on shelves along x, rows along y, all
+    top-aligned so that every open z+ face lies on the grid's z+ face (the
+    PML slab then covers the same top layers of every room); everything
+    outside the rooms is solid. In the FIXED scheme no air cell reads across
+    a wall, so each packed room evolves exactly as it does alone.
+    Returns (voxels, offsets [(ox, oy, oz)] per room)."""
+    dims = [r.shape[::-1] for r in rooms]  # (nx, ny, nz)
+    nz = max(d[2] for d in dims)
+    order = sorted(range(len(rooms)), key=lambda i: -dims[i][1])
+    width = int(np.ceil(np.sqrt(sum(d[0] * d[1] for d in dims)) * 1.3))
+    width = max(width, max(d[0] for d in dims))
+    offsets = [None] * len(rooms)
+    x = y = row_h = 0
+    for i in order:
+        nx_i, ny_i, nz_i = dims[i]
+        if x + nx_i > width:
+            x, y, row_h = 0, y + row_h, 0
+        offsets[i] = (x, y, nz - nz_i)
+        x += nx_i
+        row_h = max(row_h, ny_i)
+    gx = max(o[0] + d[0] for o, d in zip(offsets, dims))
+    gy = max(o[1] + d[1] for o, d in zip(offsets, dims))
+    vox = np.full((nz, gy, gx), filler, np.int32)
+    for r, (ox, oy, oz) in zip(rooms, offsets):
+        vox[oz:oz + r.shape[0], oy:oy + r.shape[1], ox:ox + r.shape[2]] = r
+    return vox, offsets
+
+
+def config_c3_rooms(n_rooms=8, lo=96, hi=256, steps=2048, seed=5, n_rcv=16):
+    """Uneven batch of rooms (C1 construction, edges drawn from lo..hi
+    cells): one unit-impulse source near a wall and n_rcv receivers per
+    room, all rooms packed into one grid. Returns (Config of the packed
+    grid, per-room list of (voxels, source cell, receiver cells) in room
+    coordinates, offsets)."""
+    rng = np.random.default_rng(seed)
+    a, b = passive_filters(3, 2, seed + 100)
+    rooms, parts = [], []
+    for k in range(n_rooms):
+        nx, ny, nz = (int(v) for v in rng.integers(lo, hi + 1, 3))
+        vox = room(nx, ny, nz, 63 & ~FACE_ZP, n_boxes=1, nmat=3, seed=seed + 10 + k, box_min=8,
+                   box_max=max(9, min(nx, ny, nz) // 4))
+        src = air_cells(vox, 1, seed + 200 + k, margin=2, near_wall=True)[0]
+        rcv = air_cells(vox, n_rcv, seed + 300 + k, margin=3)
+        rooms.append(vox)
+        parts.append((vox, src, rcv))
+    packed, offsets = pack_rooms(rooms)
+    gz, gy, gx = packed.shape
+    dx, c = 0.025, 343.0
+    imp = unit_impulse(1)
+    srcs, rcvs = [], []
+    for (vox, s, r), (ox, oy, oz) in zip(parts, offsets):
+        srcs.append(((s[0] + ox, s[1] + oy, s[2] + oz), imp))
+        rcvs += [(q[0] + ox, q[1] + oy, q[2] + oz) for q in r]
+    ksi = ksi_arrays((gx, gy, gz), 12, FACE_ZP)
+    cfg = Config("c3-rooms", (gx, gy, gz), packed, a, b, dx, c, courant_dt(dx, c), steps, srcs, rcvs, 12, FACE_ZP,
+                 ksi, mode=1)
+    return cfg, parts, offsets

@@ -41,8 +41,9 @@ def parse():
                     help="NX,NY,NZ: the same construction at another size (profiling captures)")
     ap.add_argument("--legs", default="device,e2e,roofline,cpu",
                     help="comma list of device,e2e,roofline,cpu")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5", "lms", "gemm"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c3rooms", "c5", "lms", "gemm"],
                     help="c2: the single-source throughput line (default); c3: batched secondary-path IRs/s; "
+                         "c3rooms: 8 uneven rooms in one launch; "
                          "c5: the learned surrogate against the FDTD; lms: LMS impulse-response estimation "
                          "at the ie224-noise size; gemm: the surrogate's tcgen05 GEMM")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
@@ -227,6 +228,68 @@ def bench_c3(pkg, args):
             "clocks": clk}
 
 
+def bench_c3_rooms(pkg, args):
+    """Uneven batch: 8 rooms (C1 construction, edges 96-256 cells, PML z+,
+    one wall-adjacent unit impulse and 16 receivers each) packed into one
+    grid and advanced by one simulation (one launch per kernel per step),
+    against the same 8 rooms run one after another. Metric: room
+    cell-updates/s (interior cells of the rooms x steps / wall seconds)."""
+    import torch
+    W = pkg.workloads
+    cfg, parts, offsets = W.config_c3_rooms()
+    steps = cfg.steps
+
+    def make(vox, dims, srcs, rcvs):
+        sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt)
+        sim.SetModel(pkg.Model.from_voxels(vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
+        sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=W.ksi_arrays(dims, cfg.pml_width, cfg.pml_faces))
+        for cell, sig in srcs:
+            sim.AddSourceCell(cell, sig)
+        for r in rcvs:
+            sim.AddMicCell(r)
+        sim.prepare(steps)
+        return sim
+
+    room_cells = sum((v.shape[0] - 2) * (v.shape[1] - 2) * (v.shape[2] - 2) for v, _, _ in parts)
+    clocks = Clocks(0)
+    clocks.start()
+    sim = make(cfg.vox, cfg.dims, cfg.sources, cfg.receivers)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    sim.Run(steps)
+    torch.cuda.synchronize()
+    t_packed = time.perf_counter() - t
+    y_packed = sim.mics()
+    sim.close()
+    t_seq, same = 0.0, True
+    n_rcv = len(parts[0][2])
+    for k, (vox, src, rcv) in enumerate(parts):
+        nz, ny, nx = vox.shape
+        s1 = make(vox, (nx, ny, nz), [(src, cfg.sources[k][1])], rcv)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        s1.Run(steps)
+        torch.cuda.synchronize()
+        t_seq += time.perf_counter() - t
+        same &= bool(np.array_equal(s1.mics(), y_packed[k * n_rcv:(k + 1) * n_rcv]))
+        s1.close()
+    clk = clocks.stop()
+    v = room_cells * steps / t_packed / 1e6
+    gx, gy, gz = cfg.dims
+    return {"metric": "Mcell-updates/s", "value": v, "unit": "Mcell-updates/s", "n_gpus": 1, "steps": steps,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "8 uneven rooms (edges 96-256, C1 construction, PML z+) packed into one "
+                                   "%dx%dx%d grid, one launch per kernel per step, %d steps" % (gx, gy, gz, steps),
+                       "room_cells": room_cells, "packed_grid_cells": gx * gy * gz,
+                       "rooms": [list(p[0].shape[::-1]) for p in parts],
+                       "each_room_equals_its_own_run": same},
+            "paths": {"packed_one_launch": {"run_s": t_packed, "mcell_per_s": v},
+                      "rooms_one_after_another": {"run_s": t_seq,
+                                                  "mcell_per_s": room_cells * steps / t_seq / 1e6}},
+            "clocks": clk}
+
+
 def bench_lms(pkg, args):
     """EstimateIr (anc_field_py/ancutil.py:24-37) at the size of
     examples/ie224-noise.py: 64000 taps, 10 s at 32 kHz (320000 samples), 16
@@ -322,7 +385,8 @@ def main():
     pkg = ge.load()
     if args.workload != "c2" and args.impl == "b200":
         if rank == 0:
-            line = {"c3": bench_c3, "c5": bench_c5, "lms": bench_lms, "gemm": bench_gemm}[args.workload](pkg, args)
+            line = {"c3": bench_c3, "c3rooms": bench_c3_rooms, "c5": bench_c5, "lms": bench_lms,
+                    "gemm": bench_gemm}[args.workload](pkg, args)
             print(json.dumps(line), flush=True)
         return
     W = pkg.workloads

@@ -83,3 +83,24 @@ def test_replica_rate():
     import bench
     # two replicas of 1e6 cells, 100 steps, slowest rank 10 ms -> 2e10 cells/s
     assert bench.replica_rate(1e6, 100, 2, 10.0) == pytest.approx(20000.0)
+
+
+def test_pack_rooms_places_rooms_without_overlap(pkg):
+    W = pkg.workloads
+    rooms = [W.room(nx, ny, nz, 63 & ~W.FACE_ZP, n_boxes=0, nmat=2, seed=k)
+             for k, (nx, ny, nz) in enumerate([(20, 16, 12), (14, 22, 9), (30, 10, 15), (12, 12, 12)])]
+    packed, offsets = W.pack_rooms(rooms, filler=1)
+    gz, gy, gx = packed.shape
+    assert gz == max(r.shape[0] for r in rooms)
+    boxes = []
+    for r, (ox, oy, oz) in zip(rooms, offsets):
+        nz, ny, nx = r.shape
+        assert oz + nz == gz  # top-aligned: every open z+ face on the grid's z+ face
+        assert np.array_equal(packed[oz:oz + nz, oy:oy + ny, ox:ox + nx], r)
+        boxes.append((ox, ox + nx, oy, oy + ny))
+    for i in range(len(boxes)):
+        for j in range(i + 1, len(boxes)):
+            a, b = boxes[i], boxes[j]
+            assert a[1] <= b[0] or b[1] <= a[0] or a[3] <= b[2] or b[3] <= a[2]
+    # every air cell of the packed grid belongs to one room
+    assert (packed == -1).sum() == sum((r == -1).sum() for r in rooms)
