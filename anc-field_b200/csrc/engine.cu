@@ -1172,6 +1172,10 @@ struct Engine::Impl {
     DBuf<int4> f_offs;
     DBuf<int> f_work;
     DBuf<int> f_items;  // compact work list of the streaming kernel (FIXED scheme)
+    std::vector<int> items_host;
+    bool items_compact = false;
+    std::array<int64_t, 6> items_key{{-1, -1, -1, -1, -1, -1}};
+    int64_t model_gen = 0;  // counts init_device calls (a new model or grid)
     CUtensorMap tm_halo{}, tm_own{};
     int fused_grid = 0;
     bool fused_dirty = true;
@@ -1357,6 +1361,7 @@ void Engine::Impl::init_device() {
     }
     initialized = true;
     fused_dirty = true;
+    ++model_gen;
 }
 
 // Work decomposition of the streaming kernel: tiles, z-chunk depth and the
@@ -1389,6 +1394,24 @@ void Engine::Impl::build_fused() {
     // every side holds no air are left out (uneven rooms packed into one
     // grid, thick walls). REF keeps every item: its X_M_Y_M_Z_M corner reads
     // solid neighbours' leapfrog values.
+    // the work list depends on the model, the tiling and the batch only
+    const std::array<int64_t, 6> key = {model_gen, tiles_x, tiles_y, dz, prm.batch, f16() ? 1 : 0};
+    if (key != items_key) {
+        items_key = key;
+        items_host.clear();
+        items_compact = false;
+    } else if (items_compact) {
+        F.items = f_items.ptr;
+        F.n_items = (int32_t)items_host.size();
+        n_items = (int64_t)items_host.size();
+        fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));
+        fused_dirty = false;
+        return;
+    } else {
+        fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));
+        fused_dirty = false;
+        return;
+    }
     f_items.release();
     if (!ref() && have_model) {
         const int W = f16() ? Tile<__half>::W : Tile<float>::W;
@@ -1421,6 +1444,8 @@ void Engine::Impl::build_fused() {
             F.items = f_items.ptr;
             F.n_items = (int32_t)items.size();
             n_items = (int64_t)items.size();
+            items_host.swap(items);
+            items_compact = true;
         }
     }
     fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));

@@ -33,7 +33,7 @@ sys.path.insert(0, ROOT)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -392,7 +392,9 @@ def main():
     W = pkg.workloads
     legs = set(args.legs.split(","))
     dims = tuple(int(v) for v in args.grid.split(",")) if args.grid else (512, 384, 320)
-    cfg = W.config_c2(steps=max(args.steps, 1), dims=dims)
+    # the source covers warm-up, the device leg and the e2e leg, so the e2e
+    # leg's per-chunk source updates land in place
+    cfg = W.config_c2(steps=max(args.warmup, 3) + 2 * max(args.steps, 1) + 400, dims=dims)
     nx, ny, nz = cfg.dims
     interior = (nx - 2) * (ny - 2) * (nz - 2)
     metric = "Mcell-updates/s"
