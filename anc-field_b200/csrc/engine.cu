@@ -791,14 +791,19 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                 v.w = slf_update(L2, CI, xp, c.z, yp.w, ym.w, zp.w, zm.w, c.w, o.w);
                 bad |= !(fabsf(v.x) < 1e30f && fabsf(v.y) < 1e30f && fabsf(v.z) < 1e30f && fabsf(v.w) < 1e30f);
                 if (yok) {
+                    // cells owned by the boundary/PML kernels are left to them
+                    const unsigned own =
+                        f.owned && x <= a.g.nx - 2
+                            ? (__ldg(f.owned + ((int64_t)z * a.g.ny + y) * f.owned_wpr + (x >> 5)) >> (x & 31)) & 0xFu
+                            : 0u;
                     float* dst = pn + (int64_t)z * a.g.plane;
-                    if (xfull) {
+                    if (xfull && !own) {
                         __stcs(reinterpret_cast<float4*>(dst), v);
                     } else {
                         const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                         for (int m = 0; m < 4; ++m)
-                            if (x + m >= 1 && x + m <= a.g.nx - 2) dst[m] = vv[m];
+                            if (x + m >= 1 && x + m <= a.g.nx - 2 && !((own >> m) & 1u)) dst[m] = vv[m];
                     }
                 }
             }
@@ -876,13 +881,17 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                     omax = __vmaxu2(omax, outw[w] & 0x7fff7fffu);
                 }
                 if (yok) {
+                    const unsigned own =
+                        f.owned && x <= a.g.nx - 2
+                            ? (__ldg(f.owned + ((int64_t)z * a.g.ny + y) * f.owned_wpr + (x >> 5)) >> (x & 31)) & 0xFFu
+                            : 0u;
                     __half* dst = pn + (int64_t)z * a.g.plane;
-                    if (xfull) {
+                    if (xfull && !own) {
                         __stcs(reinterpret_cast<uint4*>(dst), make_uint4(outw[0], outw[1], outw[2], outw[3]));
                     } else {
 #pragma unroll
                         for (int m = 0; m < 8; ++m)
-                            if (x + m >= 1 && x + m <= a.g.nx - 2)
+                            if (x + m >= 1 && x + m <= a.g.nx - 2 && !((own >> m) & 1u))
                                 reinterpret_cast<unsigned short*>(dst)[m] =
                                     (unsigned short)(outw[m >> 1] >> (16 * (m & 1)));
                     }
@@ -1171,13 +1180,69 @@ struct Engine::Impl {
     FusedDev fdev{};
     DBuf<int4> f_offs;
     DBuf<int> f_work;
-    DBuf<int> f_items;  // compact work list of the streaming kernel (FIXED scheme)
-    std::vector<int> items_host;
-    bool items_compact = false;
-    std::array<int64_t, 6> items_key{{-1, -1, -1, -1, -1, -1}};
+    // compact work lists of the streaming kernel (FIXED scheme), one per plan
+    struct PlanItems {
+        std::array<int64_t, 6> key{{-1, -1, -1, -1, -1, -1}};
+        int64_t n = -1;  // -1: every item
+        DBuf<int> buf;
+    };
+    std::map<int, PlanItems> plan_items;
+    // FIXED scheme: 1 bit per cell for the cells whose new value comes from
+    // the boundary or PML kernels, which the streaming kernel then skips so
+    // that those kernels can run beside it
+    std::vector<uint32_t> pml_owned;
+    DBuf<uint32_t> owned;
+    bool owned_dirty = true;
+    // streaming plan: resident blocks per SM (0: as many as fit) and z-chunk
+    // depth (0: the rule in build_fused); the online autotuner picks them
+    struct Plan {
+        int per_sm, dz;
+        bool beside;  // boundary and PML pressure kernels beside the streaming kernel
+    };
+    Plan plan{0, 0, false};
+    std::vector<Plan> tune_cands;
+    std::vector<float> tune_ms;
+    size_t tune_next = 0;
+    bool tuned = false;
+    int plan_id = 0;             // index of `plan` in tune_cands (graph cache key), 0 before tuning
+    int64_t tune_gen = -1;       // model_gen the candidates were made for
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;
+    bool tune_active() const { return use_fused() && prm.graphs && !prm.profile && !tuned; }
+    void apply_plan(int id) {
+        plan = id == 0 ? Plan{0, 0, false} : tune_cands[(size_t)id - 1];
+        plan_id = id;
+        fused_dirty = true;
+        build_fused();
+    }
+    // candidates: the streaming kernel alone with all resident blocks per SM
+    // and z-chunk depth {rule, rule / 2}, or beside the boundary and PML
+    // kernels with {all, all - 1} blocks per SM; every plan gives identical
+    // results
+    void make_candidates() {
+        tune_cands.clear();
+        auto add = [&](int ps, int d, bool bs) {
+            if (ps < 1 || d < 8) return;
+            for (const Plan& q : tune_cands)
+                if (q.per_sm == ps && q.dz == d && q.beside == bs) return;
+            tune_cands.push_back(Plan{ps, d, bs});
+        };
+        add(max_per_sm, rule_dz, false);
+        add(max_per_sm, rule_dz / 2, false);
+        if (owned.ptr && !ref()) {
+            add(max_per_sm, rule_dz, true);
+            add(max_per_sm - 1, rule_dz, true);
+        }
+        tune_ms.assign(tune_cands.size(), 0.0f);
+        tune_next = 0;
+        tuned = false;
+        tune_gen = model_gen;
+    }
+    std::vector<uint8_t> air_flags;  // [z][tile] air within the widened footprint (per model and tiling)
+    std::array<int64_t, 4> flags_key{{-1, -1, -1, -1}};
     int64_t model_gen = 0;  // counts init_device calls (a new model or grid)
     CUtensorMap tm_halo{}, tm_own{};
     int fused_grid = 0;
+    int max_per_sm = 0, rule_dz = 0;
     bool fused_dirty = true;
     int tiles_x = 0, tiles_y = 0;
 
@@ -1226,6 +1291,11 @@ struct Engine::Impl {
     void init_device();
     void build_fused();
     bool use_fused() const { return prm.fused != 0; }
+    // FIXED scheme in graphs: the boundary and PML pressure kernels run
+    // beside the streaming kernel (which skips the cells they own)
+    bool lists_beside() const {
+        return plan.beside && !ref() && use_fused() && prm.graphs && !prm.profile && owned.ptr;
+    }
     int64_t tile_key(int x, int y, int z) const {
         return ((int64_t)(y / FT_Y) * tiles_x + x / FT_X) * nz + z;
     }
@@ -1269,6 +1339,7 @@ struct Engine::Impl {
     cudaGraphExec_t graph_for(int64_t n);
     void run_chunk(int64_t n);
     void setup_run(int64_t steps);
+    void build_owned_mask();
     void collect_profile();
 };
 
@@ -1361,7 +1432,26 @@ void Engine::Impl::init_device() {
     }
     initialized = true;
     fused_dirty = true;
+    owned_dirty = true;
     ++model_gen;
+}
+
+// The owned-cell mask of the FIXED scheme: boundary cells and PML cells.
+void Engine::Impl::build_owned_mask() {
+    owned.release();
+    owned_dirty = false;
+    fused_dirty = true;
+    if (ref()) return;
+    const size_t wpr = (size_t)(pitch / 32);
+    std::vector<uint32_t> m = pml_owned.size() == (size_t)nz * ny * wpr ? pml_owned
+                                                                       : std::vector<uint32_t>((size_t)nz * ny * wpr, 0u);
+    bool any = false;
+    for (uint32_t w : m) any |= w != 0;
+    for (const BoundaryPoint& bp : boundary) {
+        m[((size_t)bp.z * ny + bp.y) * wpr + (bp.x >> 5)] |= 1u << (bp.x & 31);
+        any = true;
+    }
+    if (any) owned.upload(m);
 }
 
 // Work decomposition of the streaming kernel: tiles, z-chunk depth and the
@@ -1378,12 +1468,20 @@ void Engine::Impl::build_fused() {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, F_THREADS, smem));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    // with the boundary and PML kernels beside it, one block slot per SM is
+    // left free for them
+    max_per_sm = std::max(per_sm, 1);
+    if (plan.per_sm > 0) per_sm = std::min(per_sm, plan.per_sm);
     const int64_t resident = (int64_t)std::max(per_sm, 1) * sms;
+    F.owned = lists_beside() ? owned.ptr : nullptr;
+    F.owned_wpr = (int32_t)(pitch / 32);
     const int64_t tiles = (int64_t)tiles_x * tiles_y * prm.batch;
     // z-chunk depth: enough work items for every resident block to take a
     // few, with the two halo planes a small share of each chunk
     int dz = 64;
     while (dz > 8 && tiles * ((nz - 2 + dz - 1) / dz) < 4 * resident) dz /= 2;
+    rule_dz = dz;
+    if (plan.dz > 0) dz = plan.dz;
     F.dz = dz;
     F.n_chunks = (nz - 2 + dz - 1) / dz;
     if (!f_work.ptr) f_work.alloc(256);
@@ -1394,40 +1492,32 @@ void Engine::Impl::build_fused() {
     // every side holds no air are left out (uneven rooms packed into one
     // grid, thick walls). REF keeps every item: its X_M_Y_M_Z_M corner reads
     // solid neighbours' leapfrog values.
-    // the work list depends on the model, the tiling and the batch only
+    // the work list depends on the model, the tiling, the batch and the
+    // plan's z-chunk depth; one device copy per plan lives as long as the
+    // engine, because the graphs of every tried plan keep its address
     const std::array<int64_t, 6> key = {model_gen, tiles_x, tiles_y, dz, prm.batch, f16() ? 1 : 0};
-    if (key != items_key) {
-        items_key = key;
-        items_host.clear();
-        items_compact = false;
-    } else if (items_compact) {
-        F.items = f_items.ptr;
-        F.n_items = (int32_t)items_host.size();
-        n_items = (int64_t)items_host.size();
-        fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));
-        fused_dirty = false;
-        return;
-    } else {
-        fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));
-        fused_dirty = false;
-        return;
-    }
-    f_items.release();
-    if (!ref() && have_model) {
+    PlanItems& pi = plan_items[plan_id];
+    if (pi.key != key && !ref() && have_model) {
+        pi.key = key;
+        pi.n = -1;
         const int W = f16() ? Tile<__half>::W : Tile<float>::W;
         const int64_t ntile = (int64_t)tiles_x * tiles_y;
-        std::vector<uint8_t> flag((size_t)(ntile * nz), 0);  // [z][tile]: air within the widened footprint
-        for (int z = 0; z < nz; ++z)
-            for (int y = 0; y < ny; ++y) {
-                const int ty0 = std::max(0, (y - 1) / FT_Y), ty1 = std::min(tiles_y - 1, (y + 1) / FT_Y);
-                for (int x = 0; x < nx; ++x) {
-                    const bool air = x >= model.nx || y >= model.ny || z >= model.nz || model.at(x, y, z) == -1;
-                    if (!air) continue;
-                    const int tx0 = std::max(0, (x - 1) / W), tx1 = std::min(tiles_x - 1, (x + 1) / W);
-                    for (int ty = ty0; ty <= ty1; ++ty)
-                        for (int tx = tx0; tx <= tx1; ++tx) flag[(size_t)z * ntile + ty * tiles_x + tx] = 1;
+        const std::array<int64_t, 4> fkey = {model_gen, tiles_x, tiles_y, W};
+        if (fkey != flags_key) {
+            flags_key = fkey;
+            air_flags.assign((size_t)(ntile * nz), 0);
+            for (int z = 0; z < nz; ++z)
+                for (int y = 0; y < ny; ++y) {
+                    const int ty0 = std::max(0, (y - 1) / FT_Y), ty1 = std::min(tiles_y - 1, (y + 1) / FT_Y);
+                    for (int x = 0; x < nx; ++x) {
+                        const bool air = x >= model.nx || y >= model.ny || z >= model.nz || model.at(x, y, z) == -1;
+                        if (!air) continue;
+                        const int tx0 = std::max(0, (x - 1) / W), tx1 = std::min(tiles_x - 1, (x + 1) / W);
+                        for (int ty = ty0; ty <= ty1; ++ty)
+                            for (int tx = tx0; tx <= tx1; ++tx) air_flags[(size_t)z * ntile + ty * tiles_x + tx] = 1;
+                    }
                 }
-            }
+        }
         std::vector<int> items;
         for (int b = 0; b < prm.batch; ++b)
             for (int c = 0; c < F.n_chunks; ++c) {
@@ -1435,18 +1525,20 @@ void Engine::Impl::build_fused() {
                 for (int64_t t = 0; t < ntile; ++t) {
                     bool need = false;
                     for (int z = std::max(0, z0 - 1); z <= std::min(z1, nz - 1) && !need; ++z)
-                        need = flag[(size_t)z * ntile + t] != 0;
+                        need = air_flags[(size_t)z * ntile + t] != 0;
                     if (need) items.push_back((int)((((int64_t)b * F.n_chunks + c) * tiles_y) * tiles_x + t));
                 }
             }
         if ((int64_t)items.size() < n_items) {
-            f_items.upload(items);
-            F.items = f_items.ptr;
-            F.n_items = (int32_t)items.size();
-            n_items = (int64_t)items.size();
-            items_host.swap(items);
-            items_compact = true;
+            if (pi.buf.ptr) throw Error(AFD_ERR_STATE, "work list of a plan changed while graphs may use it");
+            pi.buf.upload(items);
+            pi.n = (int64_t)items.size();
         }
+    }
+    if (pi.n >= 0) {
+        F.items = pi.buf.ptr;
+        F.n_items = (int32_t)pi.n;
+        n_items = pi.n;
     }
     fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(n_items, resident));
     fused_dirty = false;
@@ -1455,6 +1547,8 @@ void Engine::Impl::build_fused() {
 // SetPml (simulation.hpp:233-277) applied on the device: fresh auxiliary
 // fields, ksi profiles and, in FIXED mode, the PML cell list.
 void Engine::Impl::setup_pml() {
+    pml_owned.clear();
+    owned_dirty = true;
     for (int a = 0; a < 3; ++a) {
         fi[a][0].release();
         fi[a][1].release();
@@ -1493,6 +1587,7 @@ void Engine::Impl::setup_pml() {
         std::vector<uint8_t> is_lrs((size_t)nx * ny * nz, 0);
         for (const BoundaryPoint& bp : boundary) is_lrs[((size_t)bp.z * ny + bp.y) * nx + bp.x] = 1;
         std::vector<uint32_t> air((size_t)nz * ny * wpr, 0u);
+        pml_owned.assign((size_t)nz * ny * wpr, 0u);
         auto in_slab = [&](int x, int y, int z) {
             return ((F & AFD_FACE_XM) && x < W) || ((F & AFD_FACE_XP) && x > nx - W - 1) ||
                    ((F & AFD_FACE_YM) && y < W) || ((F & AFD_FACE_YP) && y > ny - W - 1) ||
@@ -1507,8 +1602,10 @@ void Engine::Impl::setup_pml() {
                     if (have_model && x < model.nx && y < model.ny && z < model.nz && model.at(x, y, z) != -1)
                         continue;
                     air[((size_t)z * ny + y) * wpr + (x >> 5)] |= 1u << (x & 31);
-                    if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3 && z >= 2 && z <= nz - 3 && in_slab(x, y, z))
+                    if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3 && z >= 2 && z <= nz - 3 && in_slab(x, y, z)) {
                         ++npml;
+                        pml_owned[((size_t)z * ny + y) * wpr + (x >> 5)] |= 1u << (x & 31);
+                    }
                 }
         n_pml_cells = npml;
         pml_air.upload(air);
@@ -1766,18 +1863,24 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         CK(cudaEventRecord(ev_pool[ev_kind.size() - 1].second, stream));
     };
     const dim3 blk(64, 4, 1);
-    if (use_fused()) {
-        begin(KK_FUSED);
-        k_stream<T><<<fused_grid, F_THREADS, Tile<T>::SMEM, stream>>>(tm_halo, tm_own, a, fdev, j);
-        end();
+    auto stream_launch = [&](cudaStream_t st) {
+        k_stream<T><<<fused_grid, F_THREADS, Tile<T>::SMEM, st>>>(tm_halo, tm_own, a, fdev, j);
         ++launches;
-    } else {
-        const dim3 grd((unsigned)((nx - 2 + 63) / 64), (unsigned)((ny - 2 + 3) / 4),
-                       (unsigned)((nz - 2) * prm.batch));
-        begin(KK_INTERIOR);
-        k_interior<T><<<grd, blk, 0, stream>>>(a, j);
-        end();
-        ++launches;
+    };
+    const bool beside = lists_beside() && fdev.owned;
+    if (!beside) {
+        if (use_fused()) {
+            begin(KK_FUSED);
+            stream_launch(stream);
+            end();
+        } else {
+            const dim3 grd((unsigned)((nx - 2 + 63) / 64), (unsigned)((ny - 2 + 3) / 4),
+                           (unsigned)((nz - 2) * prm.batch));
+            begin(KK_INTERIOR);
+            k_interior<T><<<grd, blk, 0, stream>>>(a, j);
+            end();
+            ++launches;
+        }
     }
     auto lrs_launch = [&](cudaStream_t st) {
         const dim3 grd((unsigned)((a.lrs.n + 255) / 256), (unsigned)prm.batch);
@@ -1820,7 +1923,23 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         ++launches;
     };
     const bool fixed_pml = !ref() && a.pml.width > 0 && a.pml.n_units > 0;
-    if (fixed_pml && !profile && prm.graphs) {  // inside CUDA graphs: no host cost per step
+    if (beside) {
+        // FIXED scheme in graphs: the streaming kernel skips the cells of
+        // the boundary and PML kernels, which run beside it (they read only
+        // levels n and n-1, filter state and the old auxiliary fields); the
+        // auxiliary updates read the new level of every cell and follow.
+        std::vector<std::function<void(cudaStream_t)>> g1, g2;
+        g1.push_back(stream_launch);
+        if (a.lrs.n > 0) g1.push_back(lrs_launch);
+        if (fixed_pml)
+            for (const PmlBox& bx : pml_boxes) g1.push_back([&, bx](cudaStream_t st) { pml_p_launch(bx, st); });
+        if (fixed_pml)
+            for (int ax = 0; ax < 3; ++ax)
+                for (const PmlBox& bx : pml_axis_boxes[ax])
+                    g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
+        run_side_by_side(g1);
+        run_side_by_side(g2);
+    } else if (fixed_pml && !profile && prm.graphs) {  // inside CUDA graphs: no host cost per step
         // FIXED scheme: the boundary update and the PML pressure boxes write
         // disjoint cells and read only levels n and n-1 and the old
         // auxiliary fields, so they run side by side; the auxiliary updates
@@ -1882,7 +2001,8 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
 }
 
 cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
-    auto it = graphs.find(n);
+    const int64_t key = n + ((int64_t)plan_id << 32);  // one graph per chunk length and streaming plan
+    auto it = graphs.find(key);
     if (it != graphs.end()) return it->second;
     cudaGraph_t graph;
     const int64_t saved = launches;
@@ -1895,7 +2015,7 @@ cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
     cudaGraphExec_t exec;
     CK(cudaGraphInstantiate(&exec, graph, 0));
     cudaGraphDestroy(graph);
-    graphs[n] = exec;
+    graphs[key] = exec;
     return exec;
 }
 
@@ -1989,6 +2109,8 @@ Engine::~Engine() {
     for (auto st : D.side) cudaStreamDestroy(st);
     for (auto e : D.side_ev) cudaEventDestroy(e);
     if (D.fork_ev) cudaEventDestroy(D.fork_ev);
+    if (D.tev0) cudaEventDestroy(D.tev0);
+    if (D.tev1) cudaEventDestroy(D.tev1);
     if (D.own_stream) cudaStreamDestroy(D.own_stream);
 }
 
@@ -2133,6 +2255,7 @@ void Engine::Impl::setup_run(int64_t steps) {
         drop_graphs();
     }
     ensure_receivers(steps_done + steps);
+    if (owned_dirty) build_owned_mask();
     if (use_fused() && fused_dirty) {
         build_fused();
         drop_graphs();
@@ -2185,6 +2308,14 @@ void Engine::prepare(int64_t steps) {
 int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     Impl& D = *d_;
     D.setup_run(steps);
+    if (D.use_fused() && D.tune_gen != D.model_gen) {
+        D.make_candidates();
+        D.apply_plan(0);
+    }
+    if (D.tune_active() && !D.tev0) {
+        CK(cudaEventCreate(&D.tev0));
+        CK(cudaEventCreate(&D.tev1));
+    }
     D.launches = 0;
     for (auto& st : D.kstats) {
         st.launches = 0;
@@ -2196,9 +2327,30 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     int64_t i = 0;
     while (i < steps) {
         const int64_t n = (i == 0) ? 1 : std::min<int64_t>(200, steps - i);
+        // online autotuning: each full chunk of the first runs uses the next
+        // candidate plan, timed on the device; then the fastest is kept
+        const bool measure = D.tune_active() && n == 200 && D.tune_next < D.tune_cands.size();
+        if (measure) {
+            D.apply_plan((int)D.tune_next + 1);
+            CK(cudaEventRecord(D.tev0, D.stream));
+        }
         D.run_chunk(n);
+        if (measure) CK(cudaEventRecord(D.tev1, D.stream));
         i += n;
         const int64_t last = i - 1;
+        if (measure) {
+            CK(cudaEventSynchronize(D.tev1));
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, D.tev0, D.tev1));
+            D.tune_ms[D.tune_next++] = ms;
+            if (D.tune_next == D.tune_cands.size()) {
+                size_t best = 0;
+                for (size_t c = 1; c < D.tune_ms.size(); ++c)
+                    if (D.tune_ms[c] < D.tune_ms[best]) best = c;
+                D.tuned = true;
+                D.apply_plan((int)best + 1);
+            }
+        }
         if (D.ref() && D.args.pml.width > 0 && last % 8000 == 0) {
             const size_t bytes = (size_t)D.vol * D.prm.batch * sizeof(float);
             for (int a = 0; a < 3; ++a)
@@ -2441,6 +2593,11 @@ void Engine::get_info(afd_info* info) {
     info->storage = D.prm.storage;
     info->last_run_ms = D.last_ms;
     info->kernel_launches = D.launches;
+    info->tile_x = D.f16() ? Tile<__half>::W : Tile<float>::W;
+    info->tile_y = FT_Y;
+    info->tile_z = D.fdev.dz;
+    info->stream_blocks = D.fused_grid;
+    info->tuned = D.tuned ? 1 : 0;
 }
 
 int Engine::kernel_stats(int32_t idx, char* name, int64_t cap, int64_t* launches, double* ms) {

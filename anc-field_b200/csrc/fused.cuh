@@ -66,6 +66,8 @@ struct FusedDev {
     int* work;          // work-item counters, one per launch of a chunk
     const int* items;   // null: every item; else the n_items items to run (ascending)
     int32_t n_items;
+    const uint32_t* owned;  // null, or 1 bit per cell ([z][y][owned_wpr] words): cells not to store
+    int32_t owned_wpr;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {

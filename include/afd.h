@@ -255,8 +255,10 @@ typedef struct afd_info {
     int32_t mode, storage;
     double last_run_ms;          /* device time of the last afd_run (CUDA events) */
     int64_t kernel_launches;     /* kernels launched by the last afd_run */
-    int32_t tile_x, tile_y, tile_z;  /* tile of the fused step kernel */
-    int32_t reserved[9];
+    int32_t tile_x, tile_y, tile_z;  /* tile (cells) and z-chunk depth of the streaming kernel's plan */
+    int32_t stream_blocks;       /* resident blocks of the streaming kernel's plan */
+    int32_t tuned;               /* 1 once the online autotuner has chosen the plan */
+    int32_t reserved[7];
 } afd_info;
 int afd_get_info(afd_sim* s, afd_info* info);
 

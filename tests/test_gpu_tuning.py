@@ -1,0 +1,37 @@
+"""The streaming plan's online autotuner and the FIXED-scheme launch order
+with the boundary and PML kernels beside the streaming kernel: a run long
+enough to try every candidate plan (and switch plans between chunks)
+equals the serial run without graphs bit for bit, in FP32 and FP16."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import small_room
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_tuned_run_equals_serial_run(pkg, storage):
+    W = pkg.workloads
+    vox, a, b = small_room(nx=96, ny=72, nz=64, K=3, seed=31)
+    vox[-1] = np.where(vox[-1] >= 0, -1, vox[-1])  # open z+ for the PML
+    vox = W.close_gaps(vox)
+    nz, ny, nx = vox.shape
+    ksi = W.ksi_arrays((nx, ny, nz), 8, W.FACE_ZP, kmax=6000.0)
+    sig = W.gaussian_pulse(1400, 32000.0)
+    out = []
+    for graphs in (1, 0):
+        sim = pkg.Simulation(mode=1, graphs=graphs, storage=storage)
+        sim.SetModel(pkg.Model.from_voxels(vox, a, b))
+        sim.SetPml(8, faces=W.FACE_ZP, ksi=ksi)
+        sim.AddSourceCell((30, 30, 20), sig)
+        for r in [(50, 40, 30), (80, 20, 55), (10, 60, 10)]:
+            sim.AddMicCell(r)
+        sim.Run(1201)
+        sim.Run(199)
+        info = sim.info()
+        assert bool(info.tuned) == bool(graphs)
+        out.append((sim.mics(), sim.field()))
+        sim.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
