@@ -118,8 +118,10 @@ __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
 // compact list.
 // KT: filter length fixed at compile time (1..4), 0 for any length.
 // T: level storage (FP16 only with the FIXED scheme).
+// Memory-latency-bound gathers: 5 blocks per SM (48 registers, no spills
+// for the FIXED variants) keep more loads in flight than 4.
 template <bool REF, int KT, typename T>
-__global__ void __launch_bounds__(256) k_lrs(const __grid_constant__ StepArgs a, int j) {
+__global__ void __launch_bounds__(256, 5) k_lrs(const __grid_constant__ StepArgs a, int j) {
     const long long g = *a.d_step + j;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.lrs.n) return;
