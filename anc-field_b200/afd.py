@@ -32,6 +32,7 @@ EXPORTS = [
     "afd_default_params", "afd_version", "afd_device_name",
     "afd_model_load_kerkythea", "afd_model_from_voxels", "afd_model_dims", "afd_model_voxels",
     "afd_model_coefs", "afd_model_material_names", "afd_model_classify", "afd_model_group_points",
+    "afd_model_load_kerkythea_on", "afd_model_boundary",
     "afd_model_last_error", "afd_model_destroy", "afd_check_filters", "afd_check_filters_static",
     "afd_create", "afd_set_min_size", "afd_load", "afd_set_model", "afd_set_pml",
     "afd_set_pml_profile", "afd_add_source", "afd_add_source_cell", "afd_add_receiver",
@@ -93,6 +94,8 @@ def library(path=LIB_PATH):
         "afd_model_material_names": (C.c_int, [vp, C.c_char_p, i64]),
         "afd_model_classify": (C.c_int, [vp, P(i64)]),
         "afd_model_group_points": (C.c_int, [vp, i32, P(i32), i64, P(i64)]),
+        "afd_model_load_kerkythea_on": (C.c_int, [P(vp), C.c_char_p, f32, i32]),
+        "afd_model_boundary": (C.c_int, [vp, i32, P(i32), i64, P(i64)]),
         "afd_model_last_error": (C.c_char_p, [vp]),
         "afd_model_destroy": (None, [vp]),
         "afd_check_filters": (C.c_int, [i32, i32, P(f64), P(f64), i32, P(i32), P(f64), P(f64)]),
@@ -160,10 +163,14 @@ class Model:
         self._h = handle
 
     @classmethod
-    def load_kerkythea(cls, path, res=0.02):
+    def load_kerkythea(cls, path, res=0.02, device=None):
+        """device=None rasterises on the host, an ordinal on that GPU."""
         L = library()
         h = C.c_void_p()
-        st = L.afd_model_load_kerkythea(C.byref(h), path.encode(), res)
+        if device is None:
+            st = L.afd_model_load_kerkythea(C.byref(h), path.encode(), res)
+        else:
+            st = L.afd_model_load_kerkythea_on(C.byref(h), path.encode(), res, device)
         if st != OK:
             raise AfdError(st, L.afd_model_last_error(None).decode())
         return cls(h)
@@ -224,6 +231,16 @@ class Model:
         out = np.empty((max(n.value, 1), 6), np.int32)
         self._check(library().afd_model_group_points(self._h, group, _ptr(out, C.c_int32), out.size,
                                                      C.byref(n)))
+        return out[:n.value]
+
+    def boundary(self, device=None):
+        """Rows (x, y, z, group, mat0, mat1, mat2) of every boundary cell in
+        z-y-x scan order, classified on the host (device=None) or a GPU."""
+        dev = -1 if device is None else int(device)
+        n = C.c_int64()
+        self._check(library().afd_model_boundary(self._h, dev, None, 0, C.byref(n)))
+        out = np.empty((max(n.value, 1), 7), np.int32)
+        self._check(library().afd_model_boundary(self._h, dev, _ptr(out, C.c_int32), out.size, C.byref(n)))
         return out[:n.value]
 
     def __del__(self):

@@ -4,15 +4,21 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/afd.h"
 #include "engine.hpp"
 #include "filters.hpp"
+#include "geometry.hpp"
 #include "model.hpp"
 
 struct afd_model {
     afd::Model m;
     std::string err;
+    // the last afd_model_boundary result (a model never changes after it is
+    // made), so that the size query and the copy classify once
+    std::vector<afd::BoundaryPoint> boundary;
+    int32_t boundary_dev = -2;  // -1 host, >= 0 device ordinal, -2 none
 };
 
 struct afd_sim {
@@ -82,6 +88,16 @@ int afd_model_load_kerkythea(afd_model** out, const char* xml_path, float res) {
     *out = nullptr;
     std::unique_ptr<afd_model> m(new afd_model);
     int st = guard(g_create_error, [&] { m->m = afd::load_kerkythea(xml_path, res); });
+    if (st != AFD_OK) return st;
+    *out = m.release();
+    return AFD_OK;
+}
+
+int afd_model_load_kerkythea_on(afd_model** out, const char* xml_path, float res, int32_t device) {
+    if (!out || !xml_path) return AFD_ERR_ARG;
+    *out = nullptr;
+    std::unique_ptr<afd_model> m(new afd_model);
+    int st = guard(g_create_error, [&] { m->m = afd::load_kerkythea_on(xml_path, res, device); });
     if (st != AFD_OK) return st;
     *out = m.release();
     return AFD_OK;
@@ -189,6 +205,26 @@ int afd_model_group_points(const afd_model* m, int32_t group, int32_t* out, int6
     });
 }
 
+int afd_model_boundary(const afd_model* m, int32_t device, int32_t* out, int64_t cap, int64_t* n_out) {
+    if (!m) return AFD_ERR_ARG;
+    afd_model* mm = const_cast<afd_model*>(m);
+    return guard(mm->err, [&] {
+        const int32_t key = device < 0 ? -1 : device;
+        if (mm->boundary_dev != key) {
+            mm->boundary_dev = -2;
+            mm->boundary = key < 0 ? afd::classify(m->m) : afd::classify_on(m->m, key);
+            mm->boundary_dev = key;
+        }
+        const std::vector<afd::BoundaryPoint>& pts = mm->boundary;
+        const int64_t n = (int64_t)pts.size();
+        if (out) {
+            if (n * 7 > cap) throw afd::Error(AFD_ERR_ARG, "output buffer too small");
+            std::memcpy(out, pts.data(), (size_t)n * sizeof(afd::BoundaryPoint));
+        }
+        if (n_out) *n_out = n;
+    });
+}
+
 const char* afd_model_last_error(const afd_model* m) {
     return m ? m->err.c_str() : g_create_error.c_str();
 }
@@ -238,8 +274,7 @@ int afd_load(afd_sim* s, const char* xml_path) {
         if (!xml_path) throw afd::Error(AFD_ERR_ARG, "null path");
         // Simulation::Load uses res_ = 0.02 from the constructor; here the
         // cell size is params.dx.
-        afd::Model m = afd::load_kerkythea(xml_path, s->eng->cell_size());
-        s->eng->set_model(m);
+        s->eng->load_kerkythea(xml_path);
     });
 }
 

@@ -23,6 +23,7 @@
 #include "device.cuh"
 #include "engine.hpp"
 #include "fused.cuh"
+#include "geometry.hpp"
 
 namespace afd {
 
@@ -46,12 +47,12 @@ struct DBuf {
         ptr = nullptr;
         n = 0;
     }
-    void alloc(size_t count) {
+    void alloc(size_t count, bool zero = true) {
         release();
         if (count == 0) return;
         CK(cudaMalloc(&ptr, count * sizeof(T)));
         n = count;
-        CK(cudaMemset(ptr, 0, count * sizeof(T)));
+        if (zero) CK(cudaMemset(ptr, 0, count * sizeof(T)));
     }
     void upload(const std::vector<T>& v) {
         alloc(v.size());
@@ -1112,7 +1113,8 @@ struct Engine::Impl {
     afd_params prm{};
     // geometry
     bool have_model = false;
-    Model model;
+    Model model;  // dimensions, materials and filters; the voxels stay on the device
+    DBuf<uint32_t> model_solid;  // solid cells of the model, rows of row_words(model.nx) words
     std::vector<BoundaryPoint> boundary;
     int32_t min_size[3] = {0, 0, 0};
     int32_t nx = 0, ny = 0, nz = 0;
@@ -1189,11 +1191,11 @@ struct Engine::Impl {
         DBuf<int> buf;
     };
     std::map<int, PlanItems> plan_items;
-    // FIXED scheme: 1 bit per cell for the cells whose new value comes from
-    // the boundary or PML kernels, which the streaming kernel then skips so
-    // that those kernels can run beside it
-    std::vector<uint32_t> pml_owned;
-    DBuf<uint32_t> owned;
+    // FIXED scheme: 1 bit per cell (rows of pitch / 32 words) for the
+    // boundary cells, the PML cells, and their union: the cells whose new
+    // value comes from the boundary or PML kernels, which the streaming
+    // kernel then skips so that those kernels can run beside it
+    DBuf<uint32_t> lrs_bits, pml_owned, owned;
     bool owned_dirty = true;
     // streaming plan: resident blocks per SM (0: as many as fit) and z-chunk
     // depth (0: the rule in build_fused); the online autotuner picks them
@@ -1240,6 +1242,17 @@ struct Engine::Impl {
         tune_gen = model_gen;
     }
     std::vector<uint8_t> air_flags;  // [z][tile] air within the widened footprint (per model and tiling)
+    SolidBits solid_view() const {
+        SolidBits sb;
+        if (have_model && model_solid.ptr) {
+            sb.bits = model_solid.ptr;
+            sb.nx = model.nx;
+            sb.ny = model.ny;
+            sb.nz = model.nz;
+            sb.w = row_words(model.nx);
+        }
+        return sb;
+    }
     std::array<int64_t, 4> flags_key{{-1, -1, -1, -1}};
     int64_t model_gen = 0;  // counts init_device calls (a new model or grid)
     CUtensorMap tm_halo{}, tm_own{};
@@ -1291,6 +1304,7 @@ struct Engine::Impl {
     }
 
     void init_device();
+    void adopt_model(Model&& hdr, const int32_t* d_vox);
     void build_fused();
     bool use_fused() const { return prm.fused != 0; }
     // FIXED scheme in graphs: the boundary and PML pressure kernels run
@@ -1298,10 +1312,10 @@ struct Engine::Impl {
     bool lists_beside() const {
         return plan.beside && !ref() && use_fused() && prm.graphs && !prm.profile && owned.ptr;
     }
+    // (FT_X x FT_Y tile, plane) of a cell, in tile-major order
     int64_t tile_key(int x, int y, int z) const {
-        return ((int64_t)(y / FT_Y) * tiles_x + x / FT_X) * nz + z;
+        return ((int64_t)(y / FT_Y) * ((nx + FT_X - 1) / FT_X) + x / FT_X) * nz + z;
     }
-    static int tile_local(int x, int y) { return (y % FT_Y) * FT_X + x % FT_X; }
     void setup_pml();
     void upload_sources();
     void ensure_receivers(int64_t t_end);
@@ -1371,20 +1385,20 @@ void Engine::Impl::init_device() {
     const int tile_w = f16() ? Tile<__half>::W : Tile<float>::W;
     tiles_x = (nx + tile_w - 1) / tile_w;
     tiles_y = (ny + FT_Y - 1) / FT_Y;
-    // boundary list, sorted by (tile, plane, position in tile) for the fused
-    // kernel; the unfused kernel takes any order
-    std::vector<size_t> order(boundary.size());
-    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
-    std::stable_sort(order.begin(), order.end(), [&](size_t p, size_t q) {
-        const BoundaryPoint &A = boundary[p], &B = boundary[q];
-        const int64_t ka = tile_key(A.x, A.y, A.z), kb = tile_key(B.x, B.y, B.z);
-        if (ka != kb) return ka < kb;
-        return tile_local(A.x, A.y) < tile_local(B.x, B.y);
-    });
-    std::vector<BoundaryPoint> sorted;
-    sorted.reserve(boundary.size());
-    for (size_t k : order) sorted.push_back(boundary[k]);
-    boundary.swap(sorted);
+    // boundary list, sorted by (tile, plane, position in tile) so that the
+    // boundary kernel's neighbour reads stay local; every order gives the
+    // same results. The list arrives in z-y-x scan order, in which the cells
+    // of one tile and plane already come by position in the tile, so a
+    // stable counting sort by tile_key suffices.
+    {
+        const int64_t nkey = (int64_t)((ny + FT_Y - 1) / FT_Y) * ((nx + FT_X - 1) / FT_X) * nz;
+        std::vector<int64_t> start((size_t)nkey + 1, 0);
+        for (const BoundaryPoint& b : boundary) start[(size_t)tile_key(b.x, b.y, b.z) + 1]++;
+        for (int64_t k = 0; k < nkey; ++k) start[(size_t)k + 1] += start[(size_t)k];
+        std::vector<BoundaryPoint> sorted(boundary.size());
+        for (const BoundaryPoint& b : boundary) sorted[(size_t)start[(size_t)tile_key(b.x, b.y, b.z)]++] = b;
+        boundary.swap(sorted);
+    }
     std::vector<int32_t> cell;
     std::vector<uint32_t> info;
     std::fill(group_counts, group_counts + kNumGroups, 0);
@@ -1398,6 +1412,9 @@ void Engine::Impl::init_device() {
     }
     lrs_cell.upload(cell);
     lrs_info.upload(info);
+    lrs_bits.alloc((size_t)nz * ny * (pitch / 32), false);
+    boundary_bits_device(lrs_cell.ptr, (int64_t)cell.size(), (int64_t)lrs_bits.n, lrs_bits.ptr, stream);
+    CK(cudaStreamSynchronize(stream));
     const int K = have_model ? model.ncoef : 1;
     const size_t S = 3 * (size_t)K;
     lrs_in.alloc(cell.size() * S * prm.batch);
@@ -1444,16 +1461,11 @@ void Engine::Impl::build_owned_mask() {
     owned_dirty = false;
     fused_dirty = true;
     if (ref()) return;
-    const size_t wpr = (size_t)(pitch / 32);
-    std::vector<uint32_t> m = pml_owned.size() == (size_t)nz * ny * wpr ? pml_owned
-                                                                       : std::vector<uint32_t>((size_t)nz * ny * wpr, 0u);
-    bool any = false;
-    for (uint32_t w : m) any |= w != 0;
-    for (const BoundaryPoint& bp : boundary) {
-        m[((size_t)bp.z * ny + bp.y) * wpr + (bp.x >> 5)] |= 1u << (bp.x & 31);
-        any = true;
-    }
-    if (any) owned.upload(m);
+    if (n_pml_cells == 0 && boundary.empty()) return;
+    const size_t words = (size_t)nz * ny * (pitch / 32);
+    owned.alloc(words, false);
+    or_masks_device(pml_owned.n == words ? pml_owned.ptr : nullptr, lrs_bits.ptr, owned.ptr, (int64_t)words, stream);
+    CK(cudaStreamSynchronize(stream));
 }
 
 // Work decomposition of the streaming kernel: tiles, z-chunk depth and the
@@ -1508,17 +1520,11 @@ void Engine::Impl::build_fused() {
         if (fkey != flags_key) {
             flags_key = fkey;
             air_flags.assign((size_t)(ntile * nz), 0);
-            for (int z = 0; z < nz; ++z)
-                for (int y = 0; y < ny; ++y) {
-                    const int ty0 = std::max(0, (y - 1) / FT_Y), ty1 = std::min(tiles_y - 1, (y + 1) / FT_Y);
-                    for (int x = 0; x < nx; ++x) {
-                        const bool air = x >= model.nx || y >= model.ny || z >= model.nz || model.at(x, y, z) == -1;
-                        if (!air) continue;
-                        const int tx0 = std::max(0, (x - 1) / W), tx1 = std::min(tiles_x - 1, (x + 1) / W);
-                        for (int ty = ty0; ty <= ty1; ++ty)
-                            for (int tx = tx0; tx <= tx1; ++tx) air_flags[(size_t)z * ntile + ty * tiles_x + tx] = 1;
-                    }
-                }
+            DBuf<uint8_t> fl;
+            fl.alloc(air_flags.size(), false);
+            air_flags_device(solid_view(), nx, ny, nz, W, FT_Y, tiles_x, tiles_y, fl.ptr, stream);
+            CK(cudaMemcpyAsync(air_flags.data(), fl.ptr, air_flags.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
         }
         std::vector<int> items;
         for (int b = 0; b < prm.batch; ++b)
@@ -1549,7 +1555,7 @@ void Engine::Impl::build_fused() {
 // SetPml (simulation.hpp:233-277) applied on the device: fresh auxiliary
 // fields, ksi profiles and, in FIXED mode, the PML cell list.
 void Engine::Impl::setup_pml() {
-    pml_owned.clear();
+    pml_owned.release();
     owned_dirty = true;
     for (int a = 0; a < 3; ++a) {
         fi[a][0].release();
@@ -1583,34 +1589,14 @@ void Engine::Impl::setup_pml() {
         // FIXED: PML cells are the plain air cells (not solid, not boundary)
         // with 2 <= x, y, z <= n-3 inside an enabled face slab. The kernels
         // walk disjoint boxes covering the slabs and test a 1-bit air mask.
+        // (both masks built on the device from the solid and boundary bits)
         const int W = pml_width;
         const uint32_t F = pml_faces;
         const int wpr = (int)(pitch / 32);
-        std::vector<uint8_t> is_lrs((size_t)nx * ny * nz, 0);
-        for (const BoundaryPoint& bp : boundary) is_lrs[((size_t)bp.z * ny + bp.y) * nx + bp.x] = 1;
-        std::vector<uint32_t> air((size_t)nz * ny * wpr, 0u);
-        pml_owned.assign((size_t)nz * ny * wpr, 0u);
-        auto in_slab = [&](int x, int y, int z) {
-            return ((F & AFD_FACE_XM) && x < W) || ((F & AFD_FACE_XP) && x > nx - W - 1) ||
-                   ((F & AFD_FACE_YM) && y < W) || ((F & AFD_FACE_YP) && y > ny - W - 1) ||
-                   ((F & AFD_FACE_ZM) && z < W) || ((F & AFD_FACE_ZP) && z > nz - W - 1);
-        };
-        int64_t npml = 0;
-        for (int z = 0; z < nz; ++z)
-            for (int y = 0; y < ny; ++y)
-                for (int x = 0; x < nx; ++x) {
-                    const size_t c = ((size_t)z * ny + y) * nx + x;
-                    if (is_lrs[c]) continue;
-                    if (have_model && x < model.nx && y < model.ny && z < model.nz && model.at(x, y, z) != -1)
-                        continue;
-                    air[((size_t)z * ny + y) * wpr + (x >> 5)] |= 1u << (x & 31);
-                    if (x >= 2 && x <= nx - 3 && y >= 2 && y <= ny - 3 && z >= 2 && z <= nz - 3 && in_slab(x, y, z)) {
-                        ++npml;
-                        pml_owned[((size_t)z * ny + y) * wpr + (x >> 5)] |= 1u << (x & 31);
-                    }
-                }
-        n_pml_cells = npml;
-        pml_air.upload(air);
+        pml_air.alloc((size_t)nz * ny * wpr, false);
+        pml_owned.alloc((size_t)nz * ny * wpr, false);
+        n_pml_cells = pml_masks_device(solid_view(), lrs_bits.ptr, nx, ny, nz, wpr, W, F, pml_air.ptr, pml_owned.ptr,
+                                       stream);
         // disjoint boxes: z slabs take whole planes, y slabs the remaining
         // planes, x slabs the remaining rows
         pml_boxes.clear();
@@ -2141,19 +2127,64 @@ void Engine::set_min_size(float x, float y, float z) {
     std::copy(out, out + 3, D.min_size);
 }
 
+static void check_model_header(const Model& m) {
+    if (m.nx < 3 || m.ny < 3 || m.nz < 3) throw Error(AFD_ERR_ARG, "model grid must be at least 3x3x3");
+    if ((int64_t)m.vox.size() != m.cells() && !m.vox.empty()) throw Error(AFD_ERR_ARG, "voxel count mismatch");
+    if (m.nmat < 1 || m.nmat > 256) throw Error(AFD_ERR_ARG, "1..256 materials are supported");
+    if (m.ncoef < 1 || m.ncoef > 64) throw Error(AFD_ERR_ARG, "filters must have 1..64 coefficients");
+}
+
+// Simulation::Load's LrsData (simulation.hpp:176): the voxel range check and
+// the boundary classification run on the device (geometry.cu).
 void Engine::set_model(const Model& m) {
     Impl& D = *d_;
     if (D.initialized) throw Error(AFD_ERR_STATE, "the model cannot change after the first run");
-    if (m.nx < 3 || m.ny < 3 || m.nz < 3) throw Error(AFD_ERR_ARG, "model grid must be at least 3x3x3");
-    if (m.nmat < 1 || m.nmat > 256) throw Error(AFD_ERR_ARG, "1..256 materials are supported");
-    if (m.ncoef < 1 || m.ncoef > 64) throw Error(AFD_ERR_ARG, "filters must have 1..64 coefficients");
-    for (int64_t k = 0; k < m.cells(); ++k)
-        if (m.vox[(size_t)k] < -1 || m.vox[(size_t)k] >= m.nmat)
-            throw Error(AFD_ERR_ARG, "voxel material index out of range");
-    std::vector<BoundaryPoint> pts = classify(m);
-    D.model = m;
-    D.boundary.swap(pts);
-    D.have_model = true;
+    check_model_header(m);
+    if (m.vox.empty()) throw Error(AFD_ERR_ARG, "voxel count mismatch");
+    CK(cudaSetDevice(D.device));
+    DBuf<int32_t> dv;
+    dv.alloc((size_t)m.cells(), false);
+    CK(cudaMemcpyAsync(dv.ptr, m.vox.data(), (size_t)m.cells() * sizeof(int32_t), cudaMemcpyHostToDevice, D.stream));
+    Model hdr;
+    hdr.nx = m.nx;
+    hdr.ny = m.ny;
+    hdr.nz = m.nz;
+    hdr.nmat = m.nmat;
+    hdr.ncoef = m.ncoef;
+    hdr.a = m.a;
+    hdr.b = m.b;
+    hdr.material_names = m.material_names;
+    D.adopt_model(std::move(hdr), dv.ptr);
+}
+
+// The boundary list and the solid bits of the voxels at d_vox (on the
+// engine's stream); the model keeps no host voxels.
+void Engine::Impl::adopt_model(Model&& hdr, const int32_t* d_vox) {
+    std::vector<BoundaryPoint> pts = classify_device(d_vox, hdr.nx, hdr.ny, hdr.nz, hdr.nmat, stream);
+    DBuf<uint32_t> bits;
+    bits.alloc((size_t)hdr.ny * hdr.nz * row_words(hdr.nx), false);
+    solid_bits_device(d_vox, hdr.nx, hdr.ny, hdr.nz, bits.ptr, stream);
+    CK(cudaStreamSynchronize(stream));
+    hdr.vox.clear();
+    model = std::move(hdr);
+    std::swap(model_solid.ptr, bits.ptr);
+    std::swap(model_solid.n, bits.n);
+    boundary.swap(pts);
+    have_model = true;
+}
+
+// Simulation::Load (simulation.hpp:173-176): the scene is parsed on the host,
+// rasterised and classified on the device.
+void Engine::load_kerkythea(const std::string& xml_path) {
+    Impl& D = *d_;
+    if (D.initialized) throw Error(AFD_ERR_STATE, "the model cannot change after the first run");
+    Scene sc = parse_kerkythea(xml_path, D.prm.dx);
+    check_model_header(sc.model);
+    CK(cudaSetDevice(D.device));
+    DBuf<int32_t> dv;
+    dv.alloc((size_t)sc.model.cells(), false);
+    rasterize_device(sc, dv.ptr, D.stream);
+    D.adopt_model(std::move(sc.model), dv.ptr);
 }
 
 void Engine::set_pml(int32_t width, uint32_t faces, const float* kx, const float* ky, const float* kz) {

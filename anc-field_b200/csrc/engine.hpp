@@ -26,6 +26,7 @@ public:
 
     void set_min_size(float x, float y, float z);
     void set_model(const Model& m);
+    void load_kerkythea(const std::string& xml_path);
     void set_pml(int32_t width, uint32_t faces, const float* kx, const float* ky, const float* kz);
     void set_pml_profile(int32_t width, const float* prof, int32_t len);
     void add_source_cell(int32_t batch, const int32_t ijk[3], const float* sig, int64_t len);

@@ -296,7 +296,7 @@ std::vector<float> read_coefficients(const std::string& path) {
     return out;
 }
 
-Model load_kerkythea(const std::string& xml_path, float res) {
+Scene parse_kerkythea(const std::string& xml_path, float res) {
     if (!(res > 0.0f)) throw Error(AFD_ERR_ARG, "cell size must be positive");
     std::vector<Box> boxes = load_boxes(xml_path);
     if (boxes.empty()) throw Error(AFD_ERR_IO, "no boxes found in " + xml_path);
@@ -307,11 +307,11 @@ Model load_kerkythea(const std::string& xml_path, float res) {
         if (b.ext[3] > max_y) max_y = b.ext[3];
         if (b.ext[5] > max_z) max_z = b.ext[5];
     }
-    Model m;
+    Scene sc;
+    Model& m = sc.model;
     m.nx = (int32_t)round_to((uint32_t)(cell_of(max_x, res) + 1), 32);
     m.ny = (int32_t)round_to((uint32_t)(cell_of(max_y, res) + 1), 32);
     m.nz = (int32_t)round_to((uint32_t)(cell_of(max_z, res) + 1), 32);
-    m.vox.assign((size_t)m.cells(), -1);
 
     std::set<std::string> names;
     for (auto& b : boxes) names.insert(b.material);
@@ -331,20 +331,38 @@ Model load_kerkythea(const std::string& xml_path, float res) {
     }
     m.nmat = (int32_t)m.material_names.size();
 
-    // Inclusive rasterisation, later boxes overwrite earlier ones
-    // (kerkythea.hpp:181-195). A box whose maximum lies below zero on some
-    // axis covers no cell.
+    // Cell ranges of the boxes in file order (kerkythea.hpp:180-195). A box
+    // whose maximum lies below zero on some axis covers no cell; the minimum
+    // was clamped at zero, and the grid ends past every maximum's cell, so
+    // every range lies inside the grid.
     for (auto& b : boxes) {
         if (b.ext[1] < 0.0f || b.ext[3] < 0.0f || b.ext[5] < 0.0f) continue;
-        int32_t mat = index.at(b.material);
-        int64_t x0 = cell_of(b.ext[0], res), x1 = cell_of(b.ext[1], res);
-        int64_t y0 = cell_of(b.ext[2], res), y1 = cell_of(b.ext[3], res);
-        int64_t z0 = cell_of(b.ext[4], res), z1 = cell_of(b.ext[5], res);
-        for (int64_t z = z0; z <= z1; ++z)
-            for (int64_t y = y0; y <= y1; ++y)
-                for (int64_t x = x0; x <= x1; ++x)
-                    m.vox[(size_t)((z * m.ny + y) * m.nx + x)] = mat;
+        BoxCells c;
+        const int32_t n[3] = {m.nx, m.ny, m.nz};
+        for (int k = 0; k < 3; ++k) {
+            c.lo[k] = (int32_t)cell_of(b.ext[2 * k], res);
+            c.hi[k] = (int32_t)cell_of(b.ext[2 * k + 1], res);
+            if (c.lo[k] < 0 || c.hi[k] >= n[k]) throw Error(AFD_ERR_IO, "box outside the grid in " + xml_path);
+        }
+        c.mat = index.at(b.material);
+        sc.boxes.push_back(c);
     }
+    return sc;
+}
+
+void rasterize_host(const Scene& sc, Model& m) {
+    m.vox.assign((size_t)m.cells(), -1);
+    // inclusive ranges, later boxes overwrite earlier ones
+    for (const BoxCells& c : sc.boxes)
+        for (int64_t z = c.lo[2]; z <= c.hi[2]; ++z)
+            for (int64_t y = c.lo[1]; y <= c.hi[1]; ++y)
+                for (int64_t x = c.lo[0]; x <= c.hi[0]; ++x) m.vox[(size_t)((z * m.ny + y) * m.nx + x)] = c.mat;
+}
+
+Model load_kerkythea(const std::string& xml_path, float res) {
+    Scene sc = parse_kerkythea(xml_path, res);
+    Model m = std::move(sc.model);
+    rasterize_host(sc, m);
     return m;
 }
 

@@ -60,7 +60,28 @@ struct Model {
     int32_t at(int64_t x, int64_t y, int64_t z) const { return vox[(z * ny + y) * nx + x]; }
 };
 
-// Kerkythea constructor, anc-field/src/kerkythea.hpp:133-196.
+// Inclusive cell ranges [lo, hi] of one box and its material index.
+struct BoxCells {
+    int32_t lo[3], hi[3];
+    int32_t mat;
+};
+
+// A parsed scene: the model with grid, materials and filter tables but no
+// voxels yet, and the cell ranges of its boxes in file order.
+struct Scene {
+    Model model;
+    std::vector<BoxCells> boxes;
+};
+
+// Kerkythea constructor up to the rasterisation, kerkythea.hpp:133-179.
+Scene parse_kerkythea(const std::string& xml_path, float res);
+
+// The rasterisation loop of kerkythea.hpp:180-195: every cell air (-1), then
+// each box's cells set to its material, later boxes overwriting earlier ones.
+void rasterize_host(const Scene& sc, Model& m);
+
+// Kerkythea constructor, kerkythea.hpp:133-196: parse_kerkythea followed by
+// rasterize_host.
 Model load_kerkythea(const std::string& xml_path, float res);
 
 // Group numbering of anc-field/src/lrs-data.hpp:53-78 (X_P=0 ... X_M_Y_M_Z_M=25).

@@ -99,6 +99,11 @@ typedef struct afd_model afd_model;
  * _b.dat are read next to the XML, one coefficient per line. */
 int afd_model_load_kerkythea(afd_model** out, const char* xml_path, float res);
 
+/* The same loader with the rasterisation (kerkythea.hpp:180-195) on CUDA
+ * device `device`: the same model, voxel for voxel. afd_load uses this form
+ * on the simulation's device. */
+int afd_model_load_kerkythea_on(afd_model** out, const char* xml_path, float res, int32_t device);
+
 /* Builds a model from a caller voxel grid (-1 air, else material index)
  * and per-material coefficients a[nmat][ncoef], b[nmat][ncoef]. */
 int afd_model_from_voxels(afd_model** out, int32_t nx, int32_t ny, int32_t nz,
@@ -121,6 +126,13 @@ int afd_model_classify(const afd_model* m, int64_t counts[AFD_NUM_GROUPS]);
  * reference's z-y-x scan order. n_out receives the point count. */
 int afd_model_group_points(const afd_model* m, int32_t group, int32_t* out,
                            int64_t cap, int64_t* n_out);
+/* The whole boundary list of lrs-data.hpp:154-210 as rows {x, y, z, group,
+ * mat0, mat1, mat2} in z-y-x scan order; cap counts int32 values, out may be
+ * NULL to query n_out. device < 0 classifies on the host, device >= 0 on that
+ * CUDA device (the classifier afd_set_model and afd_load run), with the same
+ * list, or the same AFD_ERR_GEOMETRY message naming the same cell. */
+int afd_model_boundary(const afd_model* m, int32_t device, int32_t* out, int64_t cap,
+                       int64_t* n_out);
 
 const char* afd_model_last_error(const afd_model* m);
 void afd_model_destroy(afd_model* m);
