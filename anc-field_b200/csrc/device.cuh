@@ -56,11 +56,12 @@ struct PmlDev {
     float dt, cc_dxdx, inv_dx, half_inv_dx, inv_dt2, two_dt, inv_dt;
     int32_t psi_on;    // psi is kept (REF always; FIXED with faces on all three axes)
     // FIXED mode: disjoint boxes covering the slabs, and a 1-bit mask of the
-    // plain air cells (not solid, not boundary), pitch/32 words per row
+    // PML cells (plain air, not boundary, inside 2..n-3 and an enabled
+    // slab), pitch/32 words per row
     int32_t n_boxes;
     PmlBox boxes[kMaxPmlBoxes];
     int64_t n_units;
-    const uint32_t* air;
+    const uint32_t* cells;
     int32_t words_per_row;
 };
 

@@ -2,13 +2,15 @@
 // chunked step loop (per-step launches or replayed CUDA graphs).
 //
 // Per time step (simulation.hpp:358-393) the reference runs leapfrog, 26
-// LRS groups, the PML kernel, source and mic. Here a step is either
-//   fused:   one step kernel (interior + boundary + FIXED-mode PML pressure +
-//            source + receiver) and, with a FIXED-mode PML, one kernel for
-//            the auxiliary PML fields;
-//   unfused: interior, boundary, PML and source/receiver kernels in turn.
-// REF mode with a PML always takes the unfused order, because the
-// reference PML kernel reads the boundary-updated pressure of its
+// LRS groups, the PML kernel, source and mic. Here a step is
+//   fused:   the streaming interior kernel (k_stream, TMA z-marching), then
+//            the boundary list and, in FIXED mode, the PML pressure boxes
+//            (side by side inside a CUDA graph), the per-axis PML auxiliary
+//            updates and the source/receiver kernel;
+//   unfused: one-thread-per-cell interior kernel, boundary, PML and
+//            source/receiver kernels in turn.
+// REF mode with a PML runs the reference's PML order (k_pml_ref_*), because
+// the reference PML kernel reads the boundary-updated pressure of its
 // neighbours (pml.cl:124-137).
 #include <algorithm>
 #include <array>
@@ -346,19 +348,11 @@ __device__ __forceinline__ unsigned slab_axes(const StepArgs& a, int x0, int x1,
     return ax;
 }
 
-// The four cells x..x+3 of row (y, z) that are PML cells (inside 2..n-3,
-// in an enabled slab, plain air), as a bit mask.
+// The four cells x..x+3 (x a multiple of 4) of row (y, z) that are PML
+// cells (inside 2..n-3, in an enabled slab, plain air), as a bit mask.
 __device__ __forceinline__ unsigned pml_mask4(const StepArgs& a, int x, int y, int z) {
     const PmlDev& P = a.pml;
-    const uint32_t w =
-        (__ldg(P.air + ((int64_t)z * a.g.ny + y) * P.words_per_row + (x >> 5)) >> (x & 31)) & 15u;
-    unsigned m = 0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int xx = x + q;
-        if (((w >> q) & 1u) && xx >= 2 && xx <= a.g.nx - 3 && slab_axes(a, xx, xx, y, y, z, z)) m |= 1u << q;
-    }
-    return m;
+    return (__ldg(P.cells + ((int64_t)z * a.g.ny + y) * P.words_per_row + (x >> 5)) >> (x & 31)) & 15u;
 }
 
 // Thread -> (batch member, first cell) of a box launch: x in 4-cell units,
@@ -523,6 +517,15 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
         store4(P.psi[lv] + base + i, ps, m);
     }
     float v[4];
+    // ks depends on kx only within the row: one division when the four agree
+    float ksq[4];
+    if (kxv[0] == kxv[1] && kxv[1] == kxv[2] && kxv[2] == kxv[3]) {
+        const float k0 = (kxv[0] + ky + kz) / P.two_dt;
+        ksq[0] = ksq[1] = ksq[2] = ksq[3] = k0;
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ksq[q] = (kxv[q] + ky + kz) / P.two_dt;
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float xmq = q == 0 ? xm : c[q - 1];
@@ -532,7 +535,7 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
         s6 = s6 + zp4[q];
         s6 = s6 + zm4[q];
         const float kx = kxv[q];
-        const float ks = (kx + ky + kz) / P.two_dt;
+        const float ks = ksq[q];
         const float A = P.cc_dxdx * (s6 - 6.0f * c[q]);
         const float B = P.inv_dx * d[q];
         const float C = kx * ky * kz * 0.5f * (ps[q] + pmh[q]);
@@ -1148,7 +1151,6 @@ struct Engine::Impl {
     DBuf<float> coef_a, coef_b;
     DBuf<float> fi[3][2], psi[2];
     DBuf<float> ksi_dev[3];
-    DBuf<uint32_t> pml_air;
     std::vector<PmlBox> pml_boxes;
     std::vector<PmlBox> pml_axis_boxes[3];
     int64_t pml_units = 0;
@@ -1564,7 +1566,6 @@ void Engine::Impl::setup_pml() {
     }
     psi[0].release();
     psi[1].release();
-    pml_air.release();
     pml_boxes.clear();
     for (auto& v : pml_axis_boxes) v.clear();
     pml_units = 0;
@@ -1593,10 +1594,8 @@ void Engine::Impl::setup_pml() {
         const int W = pml_width;
         const uint32_t F = pml_faces;
         const int wpr = (int)(pitch / 32);
-        pml_air.alloc((size_t)nz * ny * wpr, false);
         pml_owned.alloc((size_t)nz * ny * wpr, false);
-        n_pml_cells = pml_masks_device(solid_view(), lrs_bits.ptr, nx, ny, nz, wpr, W, F, pml_air.ptr, pml_owned.ptr,
-                                       stream);
+        n_pml_cells = pml_masks_device(solid_view(), lrs_bits.ptr, nx, ny, nz, wpr, W, F, pml_owned.ptr, stream);
         // disjoint boxes: z slabs take whole planes, y slabs the remaining
         // planes, x slabs the remaining rows
         pml_boxes.clear();
@@ -1786,7 +1785,7 @@ void Engine::Impl::build_args() {
     P.n_boxes = (int32_t)pml_boxes.size();
     for (size_t k = 0; k < pml_boxes.size(); ++k) P.boxes[k] = pml_boxes[k];
     P.n_units = pml_units;
-    P.air = pml_air.ptr;
+    P.cells = pml_owned.ptr;
     P.words_per_row = (int32_t)(pitch / 32);
     a.src.n = (int32_t)src_cell.n;
     a.src.cell = src_cell.ptr;
@@ -1881,8 +1880,8 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         ++launches;
     };
     auto shape = [&](const PmlBox& bx, dim3& grd, dim3& bk) {
-        unsigned w = 1;
-        while ((int)w < bx.units && w < 32) w <<= 1;
+        // rows of a narrow box packed side by side in a warp (no idle lanes)
+        const unsigned w = (unsigned)std::min(bx.units, 32);
         bk = dim3(w, 256 / w, 1);
         grd = dim3((unsigned)((bx.units + w - 1) / w), (unsigned)((bx.height + bk.y - 1) / bk.y),
                    (unsigned)(bx.depth * prm.batch));

@@ -477,7 +477,8 @@ def main():
         line["e2e"] = e2e_leg(sim, cfg, K, interior, world, metric)
     sim.close()
     if "roofline" in legs:
-        line["roofline"] = roofline_leg(make_sim, K, interior, 6.0 if f16 else 12.0)
+        line["roofline"] = roofline_leg(make_sim, K, interior, 6.0 if f16 else 12.0,
+                                        traffic_key=(tuple(cfg.dims), "fp16" if f16 else "fp32"))
     if rank == 0 and world == 1 and "cpu" in legs and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(cfg, 4)
     if rank == 0:
@@ -515,7 +516,13 @@ def e2e_leg(sim, cfg, K, interior, world, metric):
             "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * len(cfg.receivers)}
 
 
-def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0):
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# dominant kernel, measured with ncu on the full-size workload
+# (profiles/k_stream_dram_512x384x320_fp32.md), keyed by grid and storage.
+MEASURED_TRAFFIC = {((512, 384, 320), "fp32"): ("interior_stream", 740.42e6)}
+
+
+def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0, traffic_key=None):
     """Roofline of the dominant kernel from per-launch CUDA events. The
     interior kernel moves bytes_per_cell per interior cell: read p^n, read
     p^{n-1}, write p^{n+1} (4-byte values, or 2-byte FP16 storage)."""
@@ -530,12 +537,9 @@ def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0):
     peak, peak_kind = peaks()
     achieved = step_kernel_bytes / (avg_ms / 1e3) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        try:
-            traffic = json.load(open(tfile)).get(name + ("_fp16" if bytes_per_cell < 12 else ""))
-        except Exception:
-            traffic = None
+    known = MEASURED_TRAFFIC.get(traffic_key)
+    if known and known[0] == name:
+        traffic = known[1]
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
             "bytes_per_launch": step_kernel_bytes, "avg_launch_ms": avg_ms,
