@@ -8,13 +8,19 @@
 // Linear -> n_out samples. Weights kept in FP32 (Adam) with BF16 copies in
 // both orientations for the GEMMs; activations and their gradients in BF16.
 //
-// GEMM: C[M][N] = A[M][K] * B[N][K]^T, both operands K-major BF16, one
-// 128 x 128 output tile per CTA, K in steps of 64 through a 3-stage TMA
-// ring. Warp 0 (one thread) streams tiles, warp 1 allocates TMEM and one
-// of its threads issues tcgen05.mma (K = 16 per instruction) and commits
-// stage releases, warps 2-5 read the accumulator with tcgen05.ld and run
-// the epilogue. Every wait is bounded; on expiry the kernel records it in
-// the error flag, drains and frees TMEM.
+// GEMM: C[M][N] = A[M][K] * B[N][K]^T, both operands K-major BF16, K in
+// steps of 64 through a ring of TMA stages. Warp 0 (one thread) streams
+// tiles, warp 1 allocates TMEM and one of its threads issues tcgen05.mma
+// (K = 16 per instruction) and commits stage releases, warps 2-5 read the
+// accumulator with tcgen05.ld and run the epilogue. Two forms:
+//   k_gemm_p  N a multiple of 256: persistent, one CTA per SM looping over
+//             128 x 256 output tiles, 4-stage ring of 48 KB, two 256-column
+//             TMEM accumulators so that the epilogue of one tile overlaps
+//             the MMAs of the next;
+//   k_gemm    otherwise: one 128 x 128 tile per CTA, 3-stage ring, two CTAs
+//             per SM.
+// Every wait is bounded; on expiry the kernel records it in the error flag,
+// drains and frees TMEM.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -50,6 +56,10 @@ constexpr int TM = 128, TN = 128, TK = 64, NST = 3;
 constexpr int A_BYTES = TM * TK * 2, B_BYTES = TN * TK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int GEMM_THREADS = 192;
 constexpr size_t GEMM_SMEM = 1024 + (size_t)NST * STAGE_BYTES + 256;
+// persistent form
+constexpr int PTN = 256, PNST = 4;
+constexpr int PSTAGE = A_BYTES + 2 * B_BYTES;  // A 128 x 64, B 256 x 64 (two 128-row TMA boxes)
+constexpr size_t PGEMM_SMEM = 1024 + (size_t)PNST * PSTAGE + 256;
 
 enum Epi : int {
     EPI_F32 = 0,   // c32[row][col] = acc (+ bias[col])
@@ -69,6 +79,53 @@ struct GemmOut {
     int ldmask;
     int* flag;  // bit 0: a wait expired
 };
+
+// 32 accumulator columns col0 .. col0+31 of output row `row` through the
+// epilogue EPI.
+template <int EPI>
+__device__ __forceinline__ void epilogue32(const GemmOut& g, float v[32], int row, int col0) {
+    if (g.bias) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += __ldg(g.bias + col0 + j);
+    }
+    if constexpr (EPI == EPI_F32) {
+        float4* dst = reinterpret_cast<float4*>(g.c32 + (size_t)row * g.ldc + col0);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    } else {
+        if constexpr (EPI == EPI_RELU) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.0f);
+        } else {
+            const uint4* mk = reinterpret_cast<const uint4*>(g.mask + (size_t)row * g.ldmask + col0);
+#pragma unroll
+            for (int j4 = 0; j4 < 4; ++j4) {
+                const uint4 w = __ldg(mk + j4);
+                const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&ws[h]);
+                    if (!(__low2float(p) > 0.0f)) v[8 * j4 + 2 * h] = 0.0f;
+                    if (!(__high2float(p) > 0.0f)) v[8 * j4 + 2 * h + 1] = 0.0f;
+                }
+            }
+        }
+        uint32_t packed[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+            packed[j] = *reinterpret_cast<const uint32_t*>(&p);
+        }
+        uint4* dst = reinterpret_cast<uint4*>(g.c16 + (size_t)row * g.ld16 + col0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            dst[j] = make_uint4(packed[4 * j], packed[4 * j + 1], packed[4 * j + 2], packed[4 * j + 3]);
+        if (g.c16t) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) g.c16t[(size_t)(col0 + j) * g.ld16t + row] = __float2bfloat16_rn(v[j]);
+        }
+    }
+}
 
 // Two CTAs per SM (99 KB of shared memory and 128 TMEM columns each): one
 // CTA's epilogue and set-up overlap the other's MMAs.
@@ -150,48 +207,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 2)
             for (int c = 0; c < TN / 32; ++c) {
                 float v[32];
                 tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
-                const int col0 = n0 + 32 * c;
-                if (g.bias) {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] += __ldg(g.bias + col0 + j);
-                }
-                if constexpr (EPI == EPI_F32) {
-                    float4* dst = reinterpret_cast<float4*>(g.c32 + (size_t)row * g.ldc + col0);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-                } else {
-                    if constexpr (EPI == EPI_RELU) {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.0f);
-                    } else {
-                        const uint4* mk = reinterpret_cast<const uint4*>(g.mask + (size_t)row * g.ldmask + col0);
-#pragma unroll
-                        for (int j4 = 0; j4 < 4; ++j4) {
-                            const uint4 w = __ldg(mk + j4);
-                            const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-                            for (int h = 0; h < 4; ++h) {
-                                const __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&ws[h]);
-                                if (!(__low2float(p) > 0.0f)) v[8 * j4 + 2 * h] = 0.0f;
-                                if (!(__high2float(p) > 0.0f)) v[8 * j4 + 2 * h + 1] = 0.0f;
-                            }
-                        }
-                    }
-                    uint32_t packed[16];
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-                        packed[j] = *reinterpret_cast<const uint32_t*>(&p);
-                    }
-                    uint4* dst = reinterpret_cast<uint4*>(g.c16 + (size_t)row * g.ld16 + col0);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        dst[j] = make_uint4(packed[4 * j], packed[4 * j + 1], packed[4 * j + 2], packed[4 * j + 3]);
-                    if (g.c16t) {
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) g.c16t[(size_t)(col0 + j) * g.ld16t + row] = __float2bfloat16_rn(v[j]);
-                    }
-                }
+                epilogue32<EPI>(g, v, row, n0 + 32 * c);
             }
         }
     }
@@ -201,6 +217,152 @@ __global__ void __launch_bounds__(GEMM_THREADS, 2)
         __syncwarp();
         tc::fence_after();
         tc::tmem_dealloc(tmem, TN);
+    }
+}
+
+// Output tile t of the persistent form: groups of 16 row panels, columns
+// outer inside a group, so that the ~148 tiles in flight share their A and
+// B panels in L2.
+constexpr int RASTER_M = 16;
+__device__ __forceinline__ void tile_of(int t, int tiles_m, int tiles_n, int& m0, int& n0) {
+    const int per_group = RASTER_M * tiles_n;
+    const int first = (t / per_group) * RASTER_M;
+    const int gm = min(tiles_m - first, RASTER_M);
+    const int w = t % per_group;
+    m0 = (first + w % gm) * TM;
+    n0 = (w / gm) * PTN;
+}
+
+// Persistent form, one CTA per SM (194 KB of shared memory, all 512 TMEM
+// columns), tiles t = blockIdx.x + i gridDim.x placed by tile_of. Barrier
+// phases count uses: stage s is used for the u-th k-step of the CTA with
+// s = u mod 4, accumulator ab for the it-th tile with ab = it & 1.
+template <int EPI>
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    k_gemm_p(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const GemmOut g) {
+    extern __shared__ unsigned char raw[];
+    unsigned char* sm = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + PNST * PSTAGE);
+    uint64_t* empty = full + PNST;
+    uint64_t* acc_full = empty + PNST;   // [2] MMAs of a tile done
+    uint64_t* acc_empty = acc_full + 2;  // [2] its four epilogue warps done reading
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles_m = g.M / TM, tiles_n = g.N / PTN, tiles = tiles_m * tiles_n;
+    const int KT = g.K / TK;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < PNST; ++s) {
+            tc::bar_init(&full[s], 1);
+            tc::bar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            tc::bar_init(&acc_full[b], 1);
+            tc::bar_init(&acc_empty[b], 4);
+        }
+        tc::bar_init(drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tc::tmem_alloc(tslot, 2 * PTN);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t u = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                int m0, n0;
+                tile_of(t, tiles_m, tiles_n, m0, n0);
+                for (int kt = 0; kt < KT; ++kt, ++u) {
+                    const uint32_t s = u % PNST;
+                    if (u >= (uint32_t)PNST && !tc::bar_wait(&empty[s], ((u / PNST) - 1) & 1)) {
+                        atomicOr(g.flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* st = sm + s * PSTAGE;
+                    tc::bar_expect_tx(&full[s], PSTAGE);
+                    tc::tma_2d(st, &ta, kt * TK, m0, &full[s]);
+                    tc::tma_2d(st + A_BYTES, &tb, kt * TK, n0, &full[s]);
+                    tc::tma_2d(st + A_BYTES + B_BYTES, &tb, kt * TK, n0 + 128, &full[s]);
+                }
+            }
+            // the copies still in flight complete before the block leaves
+            for (uint32_t s = 0; s < (uint32_t)PNST && s < u; ++s) {
+                const uint32_t last = u - 1 - ((u - 1 - s) % PNST);
+                tc::bar_wait(&full[s], (last / PNST) & 1);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::bf16_f32_idesc(TM, PTN);
+            uint32_t u = 0;
+            int it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++it) {
+                const int ab = it & 1;
+                if (it >= 2 && !tc::bar_wait(&acc_empty[ab], ((it >> 1) - 1) & 1)) {
+                    atomicOr(g.flag, 1);
+                    break;
+                }
+                tc::fence_after();
+                const uint32_t d = tmem + (uint32_t)(ab * PTN);
+                for (int kt = 0; kt < KT; ++kt, ++u) {
+                    const uint32_t s = u % PNST;
+                    if (!tc::bar_wait(&full[s], (u / PNST) & 1)) {
+                        atomicOr(g.flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    const uint32_t a0 = tc::smem_u32(sm + s * PSTAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < TK / 16; ++ks)
+                        tc::umma_bf16(d, tc::sw128_kmajor_desc(a0 + ks * 32), tc::sw128_kmajor_desc(b0 + ks * 32),
+                                      idesc, (kt | ks) != 0);
+                    tc::umma_commit(&empty[s]);
+                }
+                if (ok) tc::umma_commit(&acc_full[ab]);
+            }
+            // every MMA issued has completed once this arrives
+            tc::umma_commit(drain);
+            tc::bar_wait(drain, 0);
+        }
+    } else {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 = tile rows
+        const int q = warp & 3;
+        int it = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+            const int ab = it & 1;
+            const bool ok = __all_sync(0xffffffffu, tc::bar_wait(&acc_full[ab], (it >> 1) & 1));
+            if (!ok) {
+                if (lane == 0) atomicOr(g.flag, 1);
+                break;
+            }
+            tc::fence_after();
+            int m0, n0;
+            tile_of(t, tiles_m, tiles_n, m0, n0);
+            const int row = m0 + 32 * q + lane;
+#pragma unroll 1
+            for (int c = 0; c < PTN / 32; ++c) {
+                float v[32];
+                tc::tmem_ld32(tmem + (uint32_t)(ab * PTN) + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
+                epilogue32<EPI>(g, v, row, n0 + 32 * c);
+            }
+            tc::fence_before();
+            __syncwarp();
+            if (lane == 0) tc::bar_arrive(&acc_empty[ab]);
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, 2 * PTN);
     }
 }
 
@@ -344,21 +506,49 @@ struct Gemm {
     int epi;
 };
 
-static void set_smem_attr() {
-    static bool done = false;
-    if (done) return;
-    MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
-    MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
-    MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM));
-    done = true;
+// Shared-memory limits of the GEMM kernels and the SM count, per device
+// (function attributes belong to the current device).
+struct DeviceGemm {
+    bool ready = false;
+    int sms = 0;
+};
+
+static int set_smem_attr() {
+    static DeviceGemm devs[64];
+    int dev = 0;
+    MCK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Err(AFD_ERR_ARG, "device ordinal out of range");
+    DeviceGemm& d = devs[dev];
+    if (d.ready) return d.sms;
+    const int s1 = (int)GEMM_SMEM, s2 = (int)PGEMM_SMEM;
+    MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm_p<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm_p<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm_p<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    MCK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    d.ready = true;
+    return d.sms;
 }
 
 static void launch(const Gemm& G, cudaStream_t st) {
-    const dim3 grid((unsigned)(G.o.N / TN), (unsigned)(G.o.M / TM));
-    switch (G.epi) {
-        case EPI_F32: k_gemm<EPI_F32><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
-        case EPI_RELU: k_gemm<EPI_RELU><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
-        default: k_gemm<EPI_MASK><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+    const int sms = set_smem_attr();
+    if (G.o.N % PTN == 0) {
+        const int tiles = (G.o.M / TM) * (G.o.N / PTN);
+        const unsigned grid = (unsigned)std::max(1, std::min(tiles, sms));
+        switch (G.epi) {
+            case EPI_F32: k_gemm_p<EPI_F32><<<grid, GEMM_THREADS, PGEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+            case EPI_RELU: k_gemm_p<EPI_RELU><<<grid, GEMM_THREADS, PGEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+            default: k_gemm_p<EPI_MASK><<<grid, GEMM_THREADS, PGEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+        }
+    } else {
+        const dim3 grid((unsigned)(G.o.N / TN), (unsigned)(G.o.M / TM));
+        switch (G.epi) {
+            case EPI_F32: k_gemm<EPI_F32><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+            case EPI_RELU: k_gemm<EPI_RELU><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+            default: k_gemm<EPI_MASK><<<grid, GEMM_THREADS, GEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+        }
     }
     MCK(cudaGetLastError());
 }
@@ -733,10 +923,32 @@ int afd_mlp_set_weights(afd_mlp* m, int32_t layer, const float* w, const float* 
     });
 }
 
+int afd_gemm_bf16_async(const void* a, const void* b, float* c, int32_t M, int32_t N, int32_t K, void* stream,
+                        int32_t* status) {
+    try {
+        if (!a || !b || !c || !status) throw Err(AFD_ERR_ARG, "null pointer");
+        Gemm g = make_gemm(EPI_F32, (const bf16*)a, (const bf16*)b, M, N, K, status);
+        g.o.c32 = c;
+        g.o.ldc = N;
+        launch(g, (cudaStream_t)stream);
+        return AFD_OK;
+    } catch (const Err& e) {
+        g_create_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_create_err = e.what();
+        return AFD_ERR_STATE;
+    }
+}
+
 int afd_gemm_bf16(const void* a, const void* b, float* c, int32_t M, int32_t N, int32_t K, void* stream) {
     try {
-        set_smem_attr();
-        static Dev<int> flag;  // the wait-expired flag, kept for the process
+        if (!a || !b || !c) throw Err(AFD_ERR_ARG, "null pointer");
+        int dev = 0;
+        MCK(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) throw Err(AFD_ERR_ARG, "device ordinal out of range");
+        static Dev<int> flags[64];  // the wait-expired flag of each device, kept for the process
+        Dev<int>& flag = flags[dev];
         if (!flag.p) flag.alloc(1);
         Gemm g = make_gemm(EPI_F32, (const bf16*)a, (const bf16*)b, M, N, K, flag.p);
         g.o.c32 = c;

@@ -15,7 +15,7 @@ WEIGHT, BIAS, GRAD_WEIGHT, GRAD_BIAS, FOURIER, FEATURES = 0, 1, 2, 3, 4, 5
 
 EXPORTS = ["afd_mlp_default_params", "afd_mlp_create", "afd_mlp_destroy", "afd_mlp_last_error",
            "afd_mlp_set_stream", "afd_mlp_train_step", "afd_mlp_gradients", "afd_mlp_predict", "afd_mlp_sync",
-           "afd_mlp_get", "afd_mlp_set_weights", "afd_gemm_bf16"]
+           "afd_mlp_get", "afd_mlp_set_weights", "afd_gemm_bf16", "afd_gemm_bf16_async"]
 
 
 class MlpParams(C.Structure):
@@ -46,6 +46,7 @@ def _lib():
             "afd_mlp_get": (C.c_int, [vp, i32, i32, P(f32), i64]),
             "afd_mlp_set_weights": (C.c_int, [vp, i32, P(f32), P(f32)]),
             "afd_gemm_bf16": (C.c_int, [vp, vp, vp, i32, i32, i32, vp]),
+            "afd_gemm_bf16_async": (C.c_int, [vp, vp, vp, i32, i32, i32, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -167,6 +168,20 @@ def gemm_bf16(a, b, c, stream=0):
     L = _lib()
     st = L.afd_gemm_bf16(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), C.c_void_p(c.data_ptr()), M, N, K,
                          C.c_void_p(stream))
+    if st != afd.OK:
+        raise afd.AfdError(st, L.afd_mlp_last_error(None).decode())
+    return c
+
+
+def gemm_bf16_async(a, b, c, status, stream=0):
+    """The same GEMM queued on `stream` without synchronising; a pipeline
+    wait that expired ORs 1 into status (an int32 device tensor of one
+    element, zeroed by the caller)."""
+    M, K = a.shape
+    N = b.shape[0]
+    L = _lib()
+    st = L.afd_gemm_bf16_async(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), C.c_void_p(c.data_ptr()), M, N,
+                               K, C.c_void_p(stream), C.c_void_p(status.data_ptr()))
     if st != afd.OK:
         raise afd.AfdError(st, L.afd_mlp_last_error(None).decode())
     return c

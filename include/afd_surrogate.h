@@ -66,8 +66,15 @@ int afd_mlp_get(afd_mlp* m, int32_t what, int32_t layer, float* out, int64_t cap
 int afd_mlp_set_weights(afd_mlp* m, int32_t layer, const float* w, const float* b);
 
 /* C[M][N] (FP32, device) = A[M][K] * B[N][K]^T with A and B BF16 row-major
- * device arrays (K contiguous); M, N multiples of 128, K of 64. */
+ * device arrays (K contiguous); M, N multiples of 128, K of 64. N a
+ * multiple of 256 runs the persistent 128 x 256 tile kernel. Synchronises
+ * the stream and fails if a kernel wait expired. */
 int afd_gemm_bf16(const void* a, const void* b, float* c, int32_t M, int32_t N, int32_t K, void* stream);
+/* The same GEMM queued on the stream without synchronising: a pipeline wait
+ * that expired ORs 1 into *status (a device int32 the caller zeroes and
+ * reads later). Usable inside stream capture. */
+int afd_gemm_bf16_async(const void* a, const void* b, float* c, int32_t M, int32_t N, int32_t K, void* stream,
+                        int32_t* status);
 
 #ifdef __cplusplus
 }

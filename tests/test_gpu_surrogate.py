@@ -22,8 +22,12 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
+# N a multiple of 256 takes the persistent 128 x 256 kernel (up to one CTA
+# per SM looping over tiles; 4096 x 2048 and 8192 x 2048 give every CTA two
+# and three or four tiles, so both TMEM accumulators are reused), other N
+# the 128 x 128 kernel.
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 512), (1024, 512, 256), (512, 2048, 1024),
-                                   (128, 256, 4096)])
+                                   (128, 256, 4096), (4096, 2048, 128), (8192, 2048, 64), (2048, 768, 192)])
 def test_gemm_matches_fp32_product(pkg, M, N, K):
     import torch
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
@@ -37,19 +41,45 @@ def test_gemm_matches_fp32_product(pkg, M, N, K):
     assert rel(c.cpu().numpy(), want.cpu().numpy()) < 1e-5
 
 
+def test_gemm_async_in_a_cuda_graph(pkg):
+    """The unsynchronised form queued inside stream capture and replayed."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(9)
+    a = torch.randn(512, 256, device="cuda", generator=g).to(torch.bfloat16)
+    b = torch.randn(512, 256, device="cuda", generator=g).to(torch.bfloat16)
+    c = torch.zeros(512, 512, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pkg.surrogate.gemm_bf16(a, b, c, torch.cuda.current_stream().cuda_stream)  # attributes set outside capture
+    c.zero_()
+    graph = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(graph, stream=s):
+            pkg.surrogate.gemm_bf16_async(a, b, c, status, s.cuda_stream)
+    graph.replay()
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    want = a.double() @ b.double().T
+    assert rel(c.cpu().numpy(), want.cpu().numpy()) < 1e-5
+
+
 def small_mlp(pkg, seed=3, **kw):
     p = dict(n_in=10, n_freq=64, hidden=128, n_layers=3, n_out=128, batch=128, seed=seed, fourier_sigma=1.5)
     p.update(kw)
     return pkg.surrogate.Mlp(**p)
 
 
-@pytest.mark.parametrize("n", [128, 77])
-def test_gradients_match_cpu_oracle(pkg, n):
+# wide: 256 features, 256 hidden units and outputs, so every GEMM of the
+# forward and backward passes (bias + ReLU, ReLU mask, FP32) runs in the
+# persistent 128 x 256 kernel; otherwise all run in the 128 x 128 kernel.
+@pytest.mark.parametrize("n,wide", [(128, False), (77, False), (77, True)])
+def test_gradients_match_cpu_oracle(pkg, n, wide):
     S = pkg.surrogate
-    m = small_mlp(pkg)
+    m = small_mlp(pkg, **(dict(n_freq=128, hidden=256, n_out=256) if wide else {}))
+    n_out = 256 if wide else 128
     rng = np.random.default_rng(5)
     x = rng.uniform(0, 1, (n, 10)).astype(np.float32)
-    y = (0.3 * rng.standard_normal((n, 128))).astype(np.float32)
+    y = (0.3 * rng.standard_normal((n, n_out))).astype(np.float32)
     loss = m.gradients(x, y)
     feat = m.get(S.FEATURES)[:n]
     W = m.weights()
