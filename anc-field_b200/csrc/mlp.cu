@@ -17,6 +17,11 @@
 //             128 x 256 output tiles, 4-stage ring of 48 KB, two 256-column
 //             TMEM accumulators so that the epilogue of one tile overlaps
 //             the MMAs of the next;
+//   k_gemm_pair  M and N multiples of 256: the same, by CTA pairs (clusters
+//             of two): 256 x 256 tiles, each CTA loading 128 rows of A and
+//             128 rows of B per k-step (32 KB, 6-stage ring) and the even CTA
+//             issuing tcgen05.mma.cta_group::2 M 256 N 256 over both CTAs'
+//             shared memory, so a CTA pulls a third less from L2 per FLOP;
 //   k_gemm    otherwise: one 128 x 128 tile per CTA, 3-stage ring, two CTAs
 //             per SM.
 // Every wait is bounded; on expiry the kernel records it in the error flag,
@@ -24,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -60,6 +66,10 @@ constexpr size_t GEMM_SMEM = 1024 + (size_t)NST * STAGE_BYTES + 256;
 constexpr int PTN = 256, PNST = 4;
 constexpr int PSTAGE = A_BYTES + 2 * B_BYTES;  // A 128 x 64, B 256 x 64 (two 128-row TMA boxes)
 constexpr size_t PGEMM_SMEM = 1024 + (size_t)PNST * PSTAGE + 256;
+// pair form
+constexpr int QNST = 6;
+constexpr int QSTAGE = A_BYTES + B_BYTES;  // 128 rows of A and 128 rows of B, 64 deep
+constexpr size_t QGEMM_SMEM = 1024 + (size_t)QNST * QSTAGE + 256;
 
 enum Epi : int {
     EPI_F32 = 0,   // c32[row][col] = acc (+ bias[col])
@@ -224,12 +234,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, 2)
 // outer inside a group, so that the ~148 tiles in flight share their A and
 // B panels in L2.
 constexpr int RASTER_M = 16;
-__device__ __forceinline__ void tile_of(int t, int tiles_m, int tiles_n, int& m0, int& n0) {
+__device__ __forceinline__ void tile_of(int t, int tiles_m, int tiles_n, int tile_h, int& m0, int& n0) {
     const int per_group = RASTER_M * tiles_n;
     const int first = (t / per_group) * RASTER_M;
     const int gm = min(tiles_m - first, RASTER_M);
     const int w = t % per_group;
-    m0 = (first + w % gm) * TM;
+    m0 = (first + w % gm) * tile_h;
     n0 = (w / gm) * PTN;
 }
 
@@ -275,7 +285,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             bool ok = true;
             for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 int m0, n0;
-                tile_of(t, tiles_m, tiles_n, m0, n0);
+                tile_of(t, tiles_m, tiles_n, TM, m0, n0);
                 for (int kt = 0; kt < KT; ++kt, ++u) {
                     const uint32_t s = u % PNST;
                     if (u >= (uint32_t)PNST && !tc::bar_wait(&empty[s], ((u / PNST) - 1) & 1)) {
@@ -344,7 +354,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             }
             tc::fence_after();
             int m0, n0;
-            tile_of(t, tiles_m, tiles_n, m0, n0);
+            tile_of(t, tiles_m, tiles_n, TM, m0, n0);
             const int row = m0 + 32 * q + lane;
 #pragma unroll 1
             for (int c = 0; c < PTN / 32; ++c) {
@@ -363,6 +373,149 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         __syncwarp();
         tc::fence_after();
         tc::tmem_dealloc(tmem, 2 * PTN);
+    }
+}
+
+// Pair form: clusters of two CTAs, one per SM, over 256 x 256 tiles placed
+// by tile_of (pair p takes tiles p, p + pairs, ...). Rank r loads rows
+// m0 + 128 r of A and n0 + 128 r of B into its own ring; both loads count
+// on rank 0's full barrier (64 KB per stage). Rank 0's MMA thread issues the
+// pair's MMAs and commits every stage release, accumulator completion and
+// the final drain to the barrier of the same offset in both CTAs. Each CTA's
+// epilogue drains its own TMEM rows and arrives on rank 0's acc_empty
+// (eight warps per use). Every path reaches both cluster barriers once.
+template <int EPI>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
+    k_gemm_pair(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const GemmOut g) {
+    extern __shared__ unsigned char raw[];
+    unsigned char* sm = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(sm + QNST * QSTAGE);
+    uint64_t* empty = full + QNST;
+    uint64_t* acc_full = empty + QNST;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = tc::cluster_rank();
+    const int pair = (int)(blockIdx.x >> 1), pairs = (int)(gridDim.x >> 1);
+    const int tiles_m = g.M / (2 * TM), tiles_n = g.N / PTN, tiles = tiles_m * tiles_n;
+    const int KT = g.K / TK;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < QNST; ++s) {
+            tc::bar_init(&full[s], 1);
+            tc::bar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            tc::bar_init(&acc_full[b], 1);
+            tc::bar_init(&acc_empty[b], 8);
+        }
+        tc::bar_init(drain, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) tc::tmem_alloc_pair(tslot, 2 * PTN);
+    tc::fence_before();
+    __syncthreads();
+    tc::cluster_sync();  // both CTAs' barriers initialised and TMEM allocated
+    tc::fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t u = 0;
+            bool ok = true;
+            for (int t = pair; t < tiles && ok; t += pairs) {
+                int m0, n0;
+                tile_of(t, tiles_m, tiles_n, 2 * TM, m0, n0);
+                const int am = m0 + (int)rank * TM, bn = n0 + (int)rank * TN;
+                for (int kt = 0; kt < KT; ++kt, ++u) {
+                    const uint32_t s = u % QNST;
+                    if (u >= (uint32_t)QNST && !tc::bar_wait(&empty[s], ((u / QNST) - 1) & 1)) {
+                        atomicOr(g.flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    if (rank == 0) tc::bar_expect_tx(&full[s], 2 * QSTAGE);
+                    const uint32_t fb = tc::mapa(tc::smem_u32(&full[s]), 0);
+                    unsigned char* st = sm + s * QSTAGE;
+                    tc::tma_2d_pair(st, &ta, kt * TK, am, fb);
+                    tc::tma_2d_pair(st + A_BYTES, &tb, kt * TK, bn, fb);
+                }
+            }
+            // rank 0 sees the pair's copies complete; rank 1's land on the
+            // same barriers
+            if (rank == 0)
+                for (uint32_t s = 0; s < (uint32_t)QNST && s < u; ++s) {
+                    const uint32_t last = u - 1 - ((u - 1 - s) % QNST);
+                    tc::bar_wait(&full[s], (last / QNST) & 1);
+                }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 0) {
+            const uint32_t idesc = tc::bf16_f32_idesc(2 * TM, PTN);
+            uint32_t u = 0;
+            int it = 0;
+            bool ok = true;
+            for (int t = pair; t < tiles && ok; t += pairs, ++it) {
+                const int ab = it & 1;
+                if (it >= 2 && !tc::bar_wait(&acc_empty[ab], ((it >> 1) - 1) & 1)) {
+                    atomicOr(g.flag, 1);
+                    break;
+                }
+                tc::fence_after();
+                const uint32_t d = tmem + (uint32_t)(ab * PTN);
+                for (int kt = 0; kt < KT; ++kt, ++u) {
+                    const uint32_t s = u % QNST;
+                    if (!tc::bar_wait(&full[s], (u / QNST) & 1)) {
+                        atomicOr(g.flag, 1);
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    const uint32_t a0 = tc::smem_u32(sm + s * QSTAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < TK / 16; ++ks)
+                        tc::umma_bf16_pair(d, tc::sw128_kmajor_desc(a0 + ks * 32),
+                                           tc::sw128_kmajor_desc(b0 + ks * 32), idesc, (kt | ks) != 0);
+                    tc::umma_commit_pair(&empty[s], 3);
+                }
+                if (ok) tc::umma_commit_pair(&acc_full[ab], 3);
+            }
+            tc::umma_commit_pair(drain, 3);
+        }
+    } else {
+        const int q = warp & 3;
+        int it = 0;
+        for (int t = pair; t < tiles; t += pairs, ++it) {
+            const int ab = it & 1;
+            const bool ok = __all_sync(0xffffffffu, tc::bar_wait(&acc_full[ab], (it >> 1) & 1));
+            if (!ok) {
+                if (lane == 0) atomicOr(g.flag, 1);
+                break;
+            }
+            tc::fence_after();
+            int m0, n0;
+            tile_of(t, tiles_m, tiles_n, 2 * TM, m0, n0);
+            const int row = m0 + (int)rank * TM + 32 * q + lane;
+#pragma unroll 1
+            for (int c = 0; c < PTN / 32; ++c) {
+                float v[32];
+                tc::tmem_ld32(tmem + (uint32_t)(ab * PTN) + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
+                epilogue32<EPI>(g, v, row, n0 + 32 * c);
+            }
+            tc::fence_before();
+            __syncwarp();
+            if (lane == 0) tc::bar_arrive_cluster(tc::mapa(tc::smem_u32(&acc_empty[ab]), 0));
+        }
+    }
+    // every MMA of the pair has completed (rank 0 commits the drain to both)
+    if (warp == 1 && lane == 0) tc::bar_wait(drain, 0);
+    tc::fence_before();
+    __syncthreads();
+    tc::cluster_sync();  // neither CTA leaves while the other may still use its memory
+    if (warp == 1) {
+        __syncwarp();
+        tc::fence_after();
+        tc::tmem_dealloc_pair(tmem, 2 * PTN);
     }
 }
 
@@ -513,20 +666,26 @@ struct DeviceGemm {
     int sms = 0;
 };
 
+static std::mutex g_gemm_mu;  // guards the per-device tables below
+
 static int set_smem_attr() {
     static DeviceGemm devs[64];
+    std::lock_guard<std::mutex> lock(g_gemm_mu);
     int dev = 0;
     MCK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw Err(AFD_ERR_ARG, "device ordinal out of range");
     DeviceGemm& d = devs[dev];
     if (d.ready) return d.sms;
-    const int s1 = (int)GEMM_SMEM, s2 = (int)PGEMM_SMEM;
+    const int s1 = (int)GEMM_SMEM, s2 = (int)PGEMM_SMEM, s3 = (int)QGEMM_SMEM;
     MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     MCK(cudaFuncSetAttribute((const void*)k_gemm<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     MCK(cudaFuncSetAttribute((const void*)k_gemm_p<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
     MCK(cudaFuncSetAttribute((const void*)k_gemm_p<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
     MCK(cudaFuncSetAttribute((const void*)k_gemm_p<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm_pair<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm_pair<EPI_RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    MCK(cudaFuncSetAttribute((const void*)k_gemm_pair<EPI_MASK>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     MCK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
     d.ready = true;
     return d.sms;
@@ -534,7 +693,15 @@ static int set_smem_attr() {
 
 static void launch(const Gemm& G, cudaStream_t st) {
     const int sms = set_smem_attr();
-    if (G.o.N % PTN == 0) {
+    if (G.o.M % (2 * TM) == 0 && G.o.N % PTN == 0 && sms >= 2) {
+        const int tiles = (G.o.M / (2 * TM)) * (G.o.N / PTN);
+        const unsigned grid = 2u * (unsigned)std::max(1, std::min(tiles, sms / 2));
+        switch (G.epi) {
+            case EPI_F32: k_gemm_pair<EPI_F32><<<grid, GEMM_THREADS, QGEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+            case EPI_RELU: k_gemm_pair<EPI_RELU><<<grid, GEMM_THREADS, QGEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+            default: k_gemm_pair<EPI_MASK><<<grid, GEMM_THREADS, QGEMM_SMEM, st>>>(G.ta, G.tb, G.o); break;
+        }
+    } else if (G.o.N % PTN == 0) {
         const int tiles = (G.o.M / TM) * (G.o.N / PTN);
         const unsigned grid = (unsigned)std::max(1, std::min(tiles, sms));
         switch (G.epi) {
@@ -949,11 +1116,16 @@ int afd_gemm_bf16(const void* a, const void* b, float* c, int32_t M, int32_t N, 
         if (dev < 0 || dev >= 64) throw Err(AFD_ERR_ARG, "device ordinal out of range");
         static Dev<int> flags[64];  // the wait-expired flag of each device, kept for the process
         Dev<int>& flag = flags[dev];
-        if (!flag.p) flag.alloc(1);
+        {
+            std::lock_guard<std::mutex> lock(g_gemm_mu);
+            if (!flag.p) flag.alloc(1);
+        }
         Gemm g = make_gemm(EPI_F32, (const bf16*)a, (const bf16*)b, M, N, K, flag.p);
         g.o.c32 = c;
         g.o.ldc = N;
         cudaStream_t st = (cudaStream_t)stream;
+        // one flag per device: concurrent calls on one device share it
+        MCK(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
         launch(g, st);
         int f = 0;
         MCK(cudaMemcpyAsync(&f, flag.p, 4, cudaMemcpyDeviceToHost, st));

@@ -22,12 +22,14 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-# N a multiple of 256 takes the persistent 128 x 256 kernel (up to one CTA
-# per SM looping over tiles; 4096 x 2048 and 8192 x 2048 give every CTA two
-# and three or four tiles, so both TMEM accumulators are reused), other N
-# the 128 x 128 kernel.
+# M and N multiples of 256 take the CTA-pair kernel (cta_group::2, 256 x 256
+# tiles; 4096 x 2048 and 8192 x 2048 give every pair two and three or four
+# tiles, so both TMEM accumulators are reused); other M with N a multiple of
+# 256 the persistent single-CTA 128 x 256 kernel (128 x 256 x 4096,
+# 384 x 1024, 1152 x 512); other N the 128 x 128 kernel.
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 512), (1024, 512, 256), (512, 2048, 1024),
-                                   (128, 256, 4096), (4096, 2048, 128), (8192, 2048, 64), (2048, 768, 192)])
+                                   (128, 256, 4096), (4096, 2048, 128), (8192, 2048, 64), (2048, 768, 192),
+                                   (384, 1024, 256), (1152, 512, 128)])
 def test_gemm_matches_fp32_product(pkg, M, N, K):
     import torch
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
@@ -69,9 +71,11 @@ def small_mlp(pkg, seed=3, **kw):
     return pkg.surrogate.Mlp(**p)
 
 
-# wide: 256 features, 256 hidden units and outputs, so every GEMM of the
-# forward and backward passes (bias + ReLU, ReLU mask, FP32) runs in the
-# persistent 128 x 256 kernel; otherwise all run in the 128 x 128 kernel.
+# wide: 256 features, 256 hidden units and outputs, so the GEMMs of the
+# forward and backward passes (bias + ReLU, ReLU mask, FP32) run in the
+# 128 x 256 kernels (weight gradients, M = 256: the CTA-pair kernel; the
+# others, M = 128 rows: the single-CTA one); otherwise all run in the
+# 128 x 128 kernel.
 @pytest.mark.parametrize("n,wide", [(128, False), (77, False), (77, True)])
 def test_gradients_match_cpu_oracle(pkg, n, wide):
     S = pkg.surrogate
