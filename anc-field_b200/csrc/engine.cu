@@ -1224,6 +1224,14 @@ struct Engine::Impl {
     // and z-chunk depth {rule, rule / 2}, or beside the boundary and PML
     // kernels with {all, all - 1} blocks per SM; every plan gives identical
     // results
+    // candidates of the current model and grid, made once (the plan then
+    // restarts from the default)
+    void ensure_candidates() {
+        if (use_fused() && tune_gen != model_gen) {
+            make_candidates();
+            apply_plan(0);
+        }
+    }
     void make_candidates() {
         tune_cands.clear();
         auto add = [&](int ps, int d, bool bs) {
@@ -2330,20 +2338,32 @@ static std::vector<int64_t> run_chunks(int64_t steps) {
     return out;
 }
 
+// The graphs of every chunk length of a run of `steps`, for the current
+// plan and, while the autotuner still has candidates to try, for each of
+// them, so that the run itself only replays graphs.
 void Engine::prepare(int64_t steps) {
     Impl& D = *d_;
     D.setup_run(steps);
-    if (D.prm.graphs && !D.prm.profile)
-        for (int64_t n : run_chunks(steps)) D.graph_for(n);
+    if (!D.prm.graphs || D.prm.profile) return;
+    D.ensure_candidates();
+    std::vector<int64_t> lens = run_chunks(steps);
+    std::sort(lens.begin(), lens.end());
+    lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
+    if (D.tune_active() && D.tune_next < D.tune_cands.size()) {
+        const int cur = D.plan_id;
+        for (size_t c = D.tune_next; c < D.tune_cands.size(); ++c) {
+            D.apply_plan((int)c + 1);
+            for (int64_t n : lens) D.graph_for(n);
+        }
+        D.apply_plan(cur);
+    }
+    for (int64_t n : lens) D.graph_for(n);
 }
 
 int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
     Impl& D = *d_;
     D.setup_run(steps);
-    if (D.use_fused() && D.tune_gen != D.model_gen) {
-        D.make_candidates();
-        D.apply_plan(0);
-    }
+    D.ensure_candidates();
     if (D.tune_active() && !D.tev0) {
         CK(cudaEventCreate(&D.tev0));
         CK(cudaEventCreate(&D.tev1));
