@@ -13,7 +13,8 @@
 // and R(m, m+l) = r_l(m) follows from r_l(m-1) by adding x_m x_{m+l} and
 // removing x_{m-N} x_{m+l-N}. This is the same recursion reassociated; the
 // N-tap work becomes three parallel passes per block:
-//   k_lms_y0     y0 for the block, taps split over CTAs (partial sums)
+//   k_lms_y0     y0 for the block, taps and samples split over CTAs
+//                (partial sums per tap chunk)
 //   k_lms_solve  one CTA: y0 from the partials, R by lag, the errors
 //   k_lms_update w_j <- w_j + (2 mu e_m) x_{m-j} in sample order, per tap
 // All arithmetic is FP64, as in the reference.
@@ -30,33 +31,41 @@ namespace afd {
 namespace lms {
 
 constexpr int B = 128;       // samples per block
-constexpr int J = 2048;      // taps per CTA of k_lms_y0
+constexpr int J = 4096;      // taps per CTA of k_lms_y0
+constexpr int SPC = 16;      // samples per CTA of k_lms_y0 (16 x 8 = 128 CTAs at 64000 taps)
 constexpr int Y0_THREADS = 256;
+constexpr size_t Y0_SMEM = (size_t)(2 * J + SPC) * sizeof(double);
 
+// CTA (c, g): taps j0 = c J .. j0 + J - 1 of samples k0 + g SPC .. +SPC-1.
 // xs[o + t] = x_t for 0 <= t < steps, zero elsewhere (o = N + J + B).
 __global__ void __launch_bounds__(Y0_THREADS) k_lms_y0(const double* __restrict__ w, const double* __restrict__ xs,
                                                        int64_t o, int N, int64_t k0, int nb, double* partial) {
-    __shared__ double ws[J];
-    __shared__ double xw[J + B];
-    const int j0 = blockIdx.x * J;
+    extern __shared__ double y0_smem[];
+    double* ws = y0_smem;      // [J]
+    double* xw = ws + J;       // [J + SPC - 1]
+    const int j0 = blockIdx.x * J, s0 = blockIdx.y * SPC;
+    if (s0 >= nb) return;  // whole CTA
     const int nj = min(J, N - j0);
     for (int t = threadIdx.x; t < nj; t += blockDim.x) ws[t] = w[j0 + t];
-    // x_{k-j} for k in [k0, k0+nb), j in [j0, j0+nj): indices k0 - j0 - nj + 1 .. k0 + nb - 1 - j0
-    const int64_t base = o + k0 - j0 - (J - 1);
-    for (int t = threadIdx.x; t < J + B; t += blockDim.x) xw[t] = xs[base + t];
+    // x_{k-j} for k in [k0+s0, k0+s0+SPC), j in [j0, j0+J): xw[q] = x_{k0+s0-j0-(J-1)+q}
+    const int64_t base = o + k0 + s0 - j0 - (J - 1);
+    for (int t = threadIdx.x; t < J + SPC - 1; t += blockDim.x) xw[t] = xs[base + t];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = warp; i < nb; i += Y0_THREADS / 32) {
+    for (int i = warp; i < SPC && s0 + i < nb; i += Y0_THREADS / 32) {
         double acc = 0.0;
-        // x_{k0+i-j0-jj} = xw[(J - 1) + i - jj]
+        // x_{k0+s0+i-j0-jj} = xw[(J - 1) + i - jj]
         for (int jj = lane; jj < nj; jj += 32) acc += ws[jj] * xw[(J - 1) + i - jj];
         for (int s = 16; s > 0; s >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, s);
-        if (lane == 0) partial[(size_t)blockIdx.x * B + i] = acc;
+        if (lane == 0) partial[(size_t)blockIdx.x * B + s0 + i] = acc;
     }
 }
 
 // One CTA of B threads. r_state[l]: r_l at the last sample of the previous
-// block (zero at the start of a pass).
+// block (zero at the start of a pass). The two windows of x the lag sums
+// read (x_{k0 ..}, x_{k0-N ..}, 2 B - 1 values each) are staged in shared
+// memory first, so the sequential sums wait on shared, not global, loads.
+constexpr int XW = 2 * B;  // window length (2 B - 1 used)
 __global__ void __launch_bounds__(B) k_lms_solve(const double* __restrict__ xs, int64_t o, int N, int64_t k0,
                                                  int nb, const double* __restrict__ partial, int nchunk,
                                                  const double* __restrict__ d, double mu, double* r_state,
@@ -65,29 +74,61 @@ __global__ void __launch_bounds__(B) k_lms_solve(const double* __restrict__ xs, 
     double* R = smem;          // R[i * B + l] = r_l(k0 + i)
     double* y0 = R + B * B;    // [B]
     double* e = y0 + B;        // [B]
+    double* xa = e + B;        // [XW]: x_{k0 + q}
+    double* xb = xa + XW;      // [XW]: x_{k0 - N + q}
+    double* dd = xb + XW;      // [B]: d_{k0 + i}
     const int t = threadIdx.x;
+    for (int q = t; q < nb + B - 1; q += B) {
+        xa[q] = xs[o + k0 + q];
+        xb[q] = xs[o + k0 - N + q];
+    }
     if (t < nb) {
+        dd[t] = d[k0 + t];
+        // the partials in chunk order; unrolled so that the loads overlap
         double s = 0.0;
-        for (int c = 0; c < nchunk; ++c) s += partial[(size_t)c * B + t];
+        int c = 0;
+        for (; c + 8 <= nchunk; c += 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = partial[(size_t)(c + u) * B + t];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s += v[u];
+        }
+        for (; c < nchunk; ++c) s += partial[(size_t)c * B + t];
         y0[t] = s;
     }
+    __syncthreads();
     if (t >= 1) {
         double r = r_state[t];
         for (int i = 0; i < nb; ++i) {
-            const int64_t m = o + k0 + i;
-            r += xs[m] * xs[m + t] - xs[m - N] * xs[m + t - N];
+            r += xa[i] * xa[i + t] - xb[i] * xb[i + t];
             R[i * B + t] = r;
         }
         r_state[t] = r;
     }
     __syncthreads();
+    // e_i = d_i - (y0_i + 2 mu sum_{m<i} e_m R(m, i)), forward substitution
+    // by one warp over sub-blocks of 32 samples: lane j of a sub-block first
+    // takes the earlier sub-blocks' errors, then each error of its own
+    // sub-block as the owning lane finalises it (one shuffle per sample);
+    // every sum runs in sample order.
     if (t < 32) {
         const double c2 = 2 * mu;
-        for (int i = 0; i < nb; ++i) {
+        for (int b0 = 0; b0 < nb; b0 += 32) {
+            const int j = b0 + t;
             double acc = 0.0;
-            for (int p = t; p < i; p += 32) acc += e[p] * R[p * B + (i - p)];
-            for (int s = 16; s > 0; s >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, s);
-            if (t == 0) e[i] = d[k0 + i] - (y0[i] + c2 * acc);
+            if (j < nb)
+                for (int m = 0; m < b0; ++m) acc += e[m] * R[m * B + (j - m)];
+            const int b1 = min(b0 + 32, nb);
+            for (int i = b0; i < b1; ++i) {
+                double ei = 0.0;
+                if (j == i) {
+                    ei = dd[i] - (y0[i] + c2 * acc);
+                    e[i] = ei;
+                }
+                ei = __shfl_sync(0xffffffffu, ei, i - b0);
+                if (j > i && j < nb) acc += ei * R[i * B + (j - i)];
+            }
             __syncwarp();
         }
     }
@@ -95,16 +136,25 @@ __global__ void __launch_bounds__(B) k_lms_solve(const double* __restrict__ xs, 
     if (t < nb) e_out[t] = e[t];
 }
 
-// w_j <- w_j + (2 mu e_m) x_{m-j} for the block's samples in order.
-__global__ void k_lms_update(double* w, const double* __restrict__ xs, int64_t o, int N, int64_t k0, int nb,
-                             const double* __restrict__ e_in, double mu) {
+// w_j <- w_j + (2 mu e_m) x_{m-j} for the block's samples in order. The
+// CTA's taps j0 .. j0+255 read x_{k0-j0-255} .. x_{k0-j0+nb-1}, staged in
+// shared memory first.
+constexpr int UPD_THREADS = 256;
+__global__ void __launch_bounds__(UPD_THREADS) k_lms_update(double* w, const double* __restrict__ xs, int64_t o,
+                                                            int N, int64_t k0, int nb,
+                                                            const double* __restrict__ e_in, double mu) {
     __shared__ double c[B];
-    if (threadIdx.x < nb) c[threadIdx.x] = 2 * mu * e_in[threadIdx.x];
+    __shared__ double win[UPD_THREADS + B];
+    const int tid = threadIdx.x;
+    const int j0 = blockIdx.x * UPD_THREADS;
+    if (tid < nb) c[tid] = 2 * mu * e_in[tid];
+    const int64_t base = o + k0 - j0 - (UPD_THREADS - 1);
+    for (int q = tid; q < UPD_THREADS - 1 + nb; q += UPD_THREADS) win[q] = xs[base + q];
     __syncthreads();
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = j0 + tid;
     if (j >= N) return;
     double v = w[j];
-    const double* xp = xs + o + k0 - j;
+    const double* xp = win + (UPD_THREADS - 1 - tid);  // xp[i] = x_{k0 + i - j}
     for (int i = 0; i < nb; ++i) v = v + c[i] * xp[i];
     w[j] = v;
 }
@@ -162,16 +212,20 @@ void estimate(const double* x, int64_t nx, const double* d, int64_t nd, int32_t 
     try {
         LCK(cudaMemcpyAsync(xs.p, hx.data(), nxs * sizeof(double), cudaMemcpyHostToDevice, st));
         if (steps) LCK(cudaMemcpyAsync(dd.p, d, (size_t)steps * sizeof(double), cudaMemcpyHostToDevice, st));
-        const size_t solve_smem = (size_t)(B * B + 2 * B) * sizeof(double);
+        const size_t solve_smem = (size_t)(B * B + 3 * B + 2 * XW) * sizeof(double);
         LCK(cudaFuncSetAttribute((const void*)k_lms_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)solve_smem));
+        LCK(cudaFuncSetAttribute((const void*)k_lms_y0, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Y0_SMEM));
         for (int ep = 0; ep < epochs; ++ep) {
             LCK(cudaMemsetAsync(r.p, 0, B * sizeof(double), st));  // empty delay line
             for (int64_t k0 = 0; k0 < steps; k0 += B) {
                 const int nb = (int)std::min<int64_t>(B, steps - k0);
-                k_lms_y0<<<nchunk, Y0_THREADS, 0, st>>>(w.p, xs.p, o, N, k0, nb, partial.p);
+                k_lms_y0<<<dim3((unsigned)nchunk, (unsigned)((nb + SPC - 1) / SPC)), Y0_THREADS, Y0_SMEM, st>>>(
+                    w.p, xs.p, o, N, k0, nb, partial.p);
                 k_lms_solve<<<1, B, solve_smem, st>>>(xs.p, o, N, k0, nb, partial.p, nchunk, dd.p, mu, r.p, e.p);
-                k_lms_update<<<(N + 255) / 256, 256, 0, st>>>(w.p, xs.p, o, N, k0, nb, e.p, mu);
+                k_lms_update<<<(N + UPD_THREADS - 1) / UPD_THREADS, UPD_THREADS, 0, st>>>(w.p, xs.p, o, N, k0, nb,
+                                                                                        e.p, mu);
             }
             LCK(cudaGetLastError());
         }
