@@ -46,6 +46,9 @@ def parse():
                          "c3rooms: 8 uneven rooms in one launch; "
                          "c5: the learned surrogate against the FDTD; lms: LMS impulse-response estimation "
                          "at the ie224-noise size; gemm: the surrogate's tcgen05 GEMM")
+    ap.add_argument("--shard", action="store_true",
+                    help="c3: shard the sources over the job's ranks and gather the receivers (the default "
+                         "when the job has more than one rank)")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="field storage: fp32, or fp16 levels with per-level power-of-two scales")
     return ap.parse_args()
@@ -228,6 +231,44 @@ def bench_c3(pkg, args):
             "clocks": clk}
 
 
+def bench_c3_sharded(pkg, args, rank, world, local):
+    """The batched C3 run with its 16 sources sharded over the job's ranks
+    (one GPU each, no exchange during the run) and the receiver arrays
+    gathered in source order (sharding.run_batch_sharded). IRs/s = all
+    sources x receivers / the slowest rank's device-timed run (strong
+    scaling: the total work is fixed)."""
+    import torch
+    W = pkg.workloads
+    cfg = W.config_c3()
+    steps = cfg.steps
+
+    def make_sim(batch):
+        sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, batch=batch, device=local)
+        sim.SetModel(pkg.Model.from_voxels(cfg.vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
+        sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi)
+        for r in cfg.receivers:
+            sim.AddMicCell(r)
+        return sim
+
+    clocks = Clocks(local)
+    clocks.start()
+    torch.distributed.barrier()
+    y, run_s = pkg.sharding.run_batch_sharded(pkg, make_sim, cfg.batch_sources, steps, world, rank, device="cuda")
+    clk = clocks.stop()
+    t = max_over_ranks(run_s, "cuda")
+    n_src, n_rcv = len(cfg.batch_sources), len(cfg.receivers)
+    nx, ny, nz = cfg.dims
+    return {"metric": "secondary-path IRs/s", "value": n_src * n_rcv / t, "unit": "IRs/s", "n_gpus": world,
+            "steps": steps, "warmup": 0, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%dx%dx%d room (C1 construction, PML z+), %d wall-adjacent unit-impulse sources "
+                                   "sharded over %d GPUs as batch members, %d receivers, %d steps"
+                                   % (nx, ny, nz, n_src, world, n_rcv, steps),
+                       "parallelism": "sources sharded, receivers gathered (all_gather)",
+                       "gathered": list(y.shape)},
+            "ms_per_step": t * 1e3 / steps, "clocks": clk}
+
+
 def bench_c3_rooms(pkg, args):
     """Uneven batch: 8 rooms (C1 construction, edges 96-256 cells, PML z+,
     one wall-adjacent unit impulse and 16 receivers each) packed into one
@@ -387,6 +428,18 @@ def main():
     rank, world, local = dist_env()
     import __graft_entry__ as ge
     pkg = ge.load()
+    if args.workload == "c3" and args.impl == "b200" and (world > 1 or args.shard):
+        import datetime
+        import torch
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        try:
+            line = bench_c3_sharded(pkg, args, rank, world, local)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
+        finally:
+            torch.distributed.destroy_process_group()
+        return
     if args.workload != "c2" and args.impl == "b200":
         if rank == 0:
             line = {"c3": bench_c3, "c3rooms": bench_c3_rooms, "c5": bench_c5, "lms": bench_lms,
