@@ -1119,6 +1119,7 @@ struct Engine::Impl {
     Model model;  // dimensions, materials and filters; the voxels stay on the device
     DBuf<uint32_t> model_solid;  // solid cells of the model, rows of row_words(model.nx) words
     std::vector<BoundaryPoint> boundary;
+    int64_t boundary_counts[kNumGroups] = {};  // points per group, counted when the list is set
     int32_t min_size[3] = {0, 0, 0};
     int32_t nx = 0, ny = 0, nz = 0;
     int64_t pitch = 0, plane = 0, vol = 0;
@@ -1315,6 +1316,20 @@ struct Engine::Impl {
 
     void init_device();
     void adopt_model(Model&& hdr, const int32_t* d_vox);
+    // page-locked host staging for strided device-to-host copies, grown on
+    // demand and kept for the engine's life
+    float* pinned = nullptr;
+    size_t pinned_n = 0;
+    float* pinned_floats(size_t n) {
+        if (n > pinned_n) {
+            if (pinned) cudaFreeHost(pinned);
+            pinned = nullptr;
+            pinned_n = 0;
+            CK(cudaHostAlloc((void**)&pinned, n * sizeof(float), cudaHostAllocDefault));
+            pinned_n = n;
+        }
+        return pinned;
+    }
     void build_fused();
     bool use_fused() const { return prm.fused != 0; }
     // FIXED scheme in graphs: the boundary and PML pressure kernels run
@@ -2101,6 +2116,7 @@ Engine::~Engine() {
     }
     if (D.ev0) cudaEventDestroy(D.ev0);
     if (D.ev1) cudaEventDestroy(D.ev1);
+    if (D.pinned) cudaFreeHost(D.pinned);
     for (auto st : D.side) cudaStreamDestroy(st);
     for (auto e : D.side_ev) cudaEventDestroy(e);
     if (D.fork_ev) cudaEventDestroy(D.fork_ev);
@@ -2177,6 +2193,8 @@ void Engine::Impl::adopt_model(Model&& hdr, const int32_t* d_vox) {
     std::swap(model_solid.ptr, bits.ptr);
     std::swap(model_solid.n, bits.n);
     boundary.swap(pts);
+    std::fill(boundary_counts, boundary_counts + kNumGroups, 0);
+    for (const BoundaryPoint& bp : boundary) boundary_counts[bp.group]++;
     have_model = true;
 }
 
@@ -2459,10 +2477,12 @@ void Engine::get_receivers(int32_t batch, float* out, int64_t cap) {
     if (need == 0) return;
     if (D.rcv_n_dev != nr) throw Error(AFD_ERR_STATE, "receivers were added after the last run");
     CK(cudaSetDevice(D.device));
+    float* stage = D.pinned_floats((size_t)need);
+    CK(cudaMemcpy2DAsync(stage, D.steps_done * sizeof(float),
+                         D.rcv_out.ptr + (size_t)batch * nr * D.rcv_cap, D.rcv_cap * sizeof(float),
+                         D.steps_done * sizeof(float), (size_t)nr, cudaMemcpyDeviceToHost, D.stream));
     CK(cudaStreamSynchronize(D.stream));
-    CK(cudaMemcpy2D(out, D.steps_done * sizeof(float),
-                    D.rcv_out.ptr + (size_t)batch * nr * D.rcv_cap, D.rcv_cap * sizeof(float),
-                    D.steps_done * sizeof(float), (size_t)nr, cudaMemcpyDeviceToHost));
+    std::memcpy(out, stage, (size_t)need * sizeof(float));
 }
 
 void Engine::get_receivers_range(int32_t batch, int64_t t0, int64_t t1, float* out, int64_t cap) {
@@ -2475,10 +2495,14 @@ void Engine::get_receivers_range(int32_t batch, int64_t t0, int64_t t1, float* o
     if (nr == 0 || n == 0) return;
     if (D.rcv_n_dev != nr) throw Error(AFD_ERR_STATE, "receivers were added after the last run");
     CK(cudaSetDevice(D.device));
-    CK(cudaMemcpy2DAsync(out, n * sizeof(float), D.rcv_out.ptr + (size_t)batch * nr * D.rcv_cap + t0,
+    // one strided copy into page-locked staging (a strided copy into
+    // pageable memory goes row by row), then into the caller's buffer
+    float* stage = D.pinned_floats((size_t)(nr * n));
+    CK(cudaMemcpy2DAsync(stage, n * sizeof(float), D.rcv_out.ptr + (size_t)batch * nr * D.rcv_cap + t0,
                          D.rcv_cap * sizeof(float), n * sizeof(float), (size_t)nr, cudaMemcpyDeviceToHost,
                          D.stream));
     CK(cudaStreamSynchronize(D.stream));
+    std::memcpy(out, stage, (size_t)(nr * n) * sizeof(float));
 }
 
 // Replaces samples t0.. of one source. When the device copy already holds
@@ -2636,9 +2660,7 @@ void Engine::get_info(afd_info* info) {
     info->n_sources = (int64_t)D.sources.size();
     info->n_receivers = (int64_t)D.receivers.size();
     info->n_boundary = (int64_t)D.boundary.size();
-    int64_t counts[kNumGroups] = {};
-    for (const BoundaryPoint& b : D.boundary) counts[b.group]++;
-    for (int g = 0; g < kNumGroups; ++g) info->group_counts[g] = counts[g];
+    for (int g = 0; g < kNumGroups; ++g) info->group_counts[g] = D.boundary_counts[g];
     info->n_pml_cells = D.n_pml_cells;
     info->lambda2 = D.lambda2();
     info->mode = D.prm.mode;
