@@ -255,3 +255,34 @@ def test_surrogate_rejects_untiled_sizes(pkg):
         pkg.surrogate.Mlp(hidden=100)
     assert ei.value.status == pkg.afd.ERR_ARG
     assert "multiples of 128" in str(ei.value)
+
+
+def test_gemm_entry_points_reject_bad_arguments_before_any_launch(pkg):
+    """Null pointers and untiled sizes are refused on the host (no device
+    work, so this runs without a GPU)."""
+    import ctypes as C
+    L = pkg.surrogate._lib()
+    status = C.c_int32(0)
+    assert L.afd_gemm_bf16_async(None, None, None, 128, 128, 64, None, C.byref(status)) == pkg.afd.ERR_ARG
+    assert L.afd_gemm_bf16(None, None, None, 128, 128, 64, None) == pkg.afd.ERR_ARG
+    buf = (C.c_uint16 * (128 * 64))()
+    out = (C.c_float * (128 * 128))()
+    st = L.afd_gemm_bf16_async(C.cast(buf, C.c_void_p), C.cast(buf, C.c_void_p), C.cast(out, C.c_void_p),
+                               100, 128, 64, None, C.byref(status))
+    assert st == pkg.afd.ERR_ARG
+
+
+def test_device_kerkythea_loader_reports_missing_device_or_bad_file(pkg, tmp_path):
+    import torch
+    with pytest.raises(pkg.AfdError) as ei:
+        pkg.Model.load_kerkythea(str(tmp_path / "missing.xml"), 0.02, device=0)
+    assert ei.value.status == pkg.afd.ERR_IO
+    if torch.cuda.is_available():
+        return
+    (tmp_path / "model.xml").write_text(XML.format(models=MODEL.format(name="x_m", points=box_points(
+        0, 0.1, 0, 0.1, 0, 0.1))))
+    (tmp_path / "m_a.dat").write_text("0.5\n0.1\n")
+    (tmp_path / "m_b.dat").write_text("1.0\n0.2\n")
+    with pytest.raises(pkg.AfdError) as ei:
+        pkg.Model.load_kerkythea(str(tmp_path / "model.xml"), 0.02, device=0)
+    assert ei.value.status == pkg.afd.ERR_CUDA
