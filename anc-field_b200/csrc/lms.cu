@@ -217,8 +217,10 @@ void estimate(const double* x, int64_t nx, const double* d, int64_t nd, int32_t 
                                  (int)solve_smem));
         LCK(cudaFuncSetAttribute((const void*)k_lms_y0, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)Y0_SMEM));
-        for (int ep = 0; ep < epochs; ++ep) {
-            LCK(cudaMemsetAsync(r.p, 0, B * sizeof(double), st));  // empty delay line
+        // one pass over the samples: the delay line emptied, then per block
+        // of B samples its outputs, errors and weight update
+        auto pass = [&]() {
+            LCK(cudaMemsetAsync(r.p, 0, B * sizeof(double), st));
             for (int64_t k0 = 0; k0 < steps; k0 += B) {
                 const int nb = (int)std::min<int64_t>(B, steps - k0);
                 k_lms_y0<<<dim3((unsigned)nchunk, (unsigned)((nb + SPC - 1) / SPC)), Y0_THREADS, Y0_SMEM, st>>>(
@@ -227,8 +229,38 @@ void estimate(const double* x, int64_t nx, const double* d, int64_t nd, int32_t 
                 k_lms_update<<<(N + UPD_THREADS - 1) / UPD_THREADS, UPD_THREADS, 0, st>>>(w.p, xs.p, o, N, k0, nb,
                                                                                         e.p, mu);
             }
-            LCK(cudaGetLastError());
+        };
+        if (epochs >= 2 && steps > 0) {
+            // every pass launches the same kernels with the same arguments:
+            // captured once as a graph and replayed per pass
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            LCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                pass();
+            } catch (...) {
+                cudaStreamEndCapture(st, &graph);  // leave the stream out of capture mode
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            if (ce != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                LCK(ce);
+            }
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            LCK(ie);
+            cudaError_t le = cudaSuccess;
+            for (int ep = 0; ep < epochs && le == cudaSuccess; ++ep) le = cudaGraphLaunch(exec, st);
+            const cudaError_t se = cudaStreamSynchronize(st);
+            cudaGraphExecDestroy(exec);
+            LCK(le);
+            LCK(se);
+        } else {
+            for (int ep = 0; ep < epochs; ++ep) pass();
         }
+        LCK(cudaGetLastError());
         LCK(cudaMemcpyAsync(w_out, w.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, st));
         LCK(cudaStreamSynchronize(st));
     } catch (...) {
