@@ -35,3 +35,28 @@ def test_tuned_run_equals_serial_run(pkg, storage):
         sim.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("storage", [1, 0])
+def test_tuned_batch_equals_serial_run(pkg, storage):
+    """A 16-member batch (the 256x192x160 secondary-path room, every member
+    a unit impulse at its own wall-adjacent cell): its z-chunk rule gives a
+    half-depth candidate too, and a tuned run that tries every candidate
+    equals the serial run without graphs bit for bit, member by member."""
+    W = pkg.workloads
+    cfg = W.config_c3(steps=1400)
+    out = []
+    for graphs in (1, 0):
+        sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, batch=16, graphs=graphs, storage=storage)
+        sim.SetModel(pkg.Model.from_voxels(cfg.vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
+        sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi)
+        for m in range(16):
+            for cell, sig in cfg.batch_sources[m]:
+                sim.AddSourceCell(cell, sig, batch=m)
+        for r in cfg.receivers:
+            sim.AddMicCell(r)
+        sim.Run(1400)
+        assert bool(sim.info().tuned) == bool(graphs)
+        out.append(np.stack([sim.mics(batch=m) for m in range(16)]))
+        sim.close()
+    assert np.array_equal(out[0], out[1])
