@@ -1279,6 +1279,7 @@ struct Engine::Impl {
     StepArgs args{};
     SrcRcvInline inl{};
     bool inline_ok = false;
+    bool src_beside_aux = false;  // see build_args
     std::map<int64_t, cudaGraphExec_t> graphs;
     double last_ms = 0.0;
     int64_t launches = 0;
@@ -1761,6 +1762,22 @@ void Engine::Impl::ensure_receivers(int64_t t_end) {
 }
 
 void Engine::Impl::build_args() {
+    // the source/receiver kernel may run beside the FIXED-scheme auxiliary
+    // updates when no source cell lies where they read the new pressure (a
+    // unit of 4 cells at (x, y, z) reads x..x+4, y..y+1, z..z+1): the
+    // auxiliary updates read the pressure before injection, write only the
+    // auxiliary fields, and recording reads the injected values
+    src_beside_aux = !ref() && pml_width > 0;
+    for (const Source& src : sources)
+        for (int ax = 0; ax < 3 && src_beside_aux; ++ax)
+            for (const PmlBox& bx : pml_axis_boxes[ax]) {
+                const int x = src.ijk[0], y = src.ijk[1], z = src.ijk[2];
+                if (x >= bx.x0 && x <= bx.x0 + 4 * bx.units && y >= bx.y0 && y <= bx.y0 + bx.height &&
+                    z >= bx.z0 && z <= bx.z0 + bx.depth) {
+                    src_beside_aux = false;
+                    break;
+                }
+            }
     StepArgs& a = args;
     a = StepArgs{};
     a.g = GridDev{nx, ny, nz, pitch, plane, vol};
@@ -1936,6 +1953,12 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         }
         ++launches;
     };
+    bool src_done = false;  // the source/receiver kernel already queued beside the auxiliary updates
+    auto src_rcv_launch = [&](cudaStream_t st) {
+        if (inline_ok) k_src_rcv_inline<T><<<(unsigned)prm.batch, 256, 0, st>>>(a, inl, j);
+        else k_src_rcv<T><<<(unsigned)prm.batch, 128, 0, st>>>(a, j, 1, 1);
+        ++launches;
+    };
     const bool fixed_pml = !ref() && a.pml.width > 0 && a.pml.n_units > 0;
     if (beside) {
         // FIXED scheme in graphs: the streaming kernel skips the cells of
@@ -1964,6 +1987,10 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         for (int ax = 0; ax < 3; ++ax)
             for (const PmlBox& bx : pml_axis_boxes[ax])
                 g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
+        if (src_beside_aux && (a.src.n > 0 || a.rcv.n > 0)) {
+            g2.push_back([&](cudaStream_t st) { src_rcv_launch(st); });
+            src_done = true;
+        }
         run_side_by_side(g1);
         run_side_by_side(g2);
     } else {
@@ -2000,12 +2027,10 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
             }
         }
     }
-    if (a.src.n > 0 || a.rcv.n > 0) {
+    if ((a.src.n > 0 || a.rcv.n > 0) && !src_done) {
         begin(KK_SRC_RCV);
-        if (inline_ok) k_src_rcv_inline<T><<<(unsigned)prm.batch, 256, 0, stream>>>(a, inl, j);
-        else k_src_rcv<T><<<(unsigned)prm.batch, 128, 0, stream>>>(a, j, 1, 1);
+        src_rcv_launch(stream);
         end();
-        ++launches;
     }
     if (cap_every > 0) {
         const int total = cap.rows * cap.cols;
