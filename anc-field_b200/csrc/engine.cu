@@ -1050,32 +1050,65 @@ __global__ void k_capture(const __grid_constant__ StepArgs a, const CaptureDev c
 
 __global__ void k_advance(long long* d_step, int n) { *d_step += n; }
 
-// Discrete SLF energy between the two latest levels u1 (newest) and u0,
-// in FP64: 1/2 sum (u1-u0)^2 + lambda2/2 sum over grid edges of
-// (u1_i-u1_j)(u0_i-u0_j), over the cells 1..n-2 and their edges (edges to
-// the fixed outer faces included once).
+// Solid cell of the model (cells outside the model or the grid are air).
+__device__ __forceinline__ bool cell_solid(const SolidBits& s, int x, int y, int z) {
+    if (!s.bits || x < 0 || y < 0 || z < 0 || x >= s.nx || y >= s.ny || z >= s.nz) return false;
+    return (__ldg(s.bits + ((int64_t)z * s.ny + y) * s.w + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+// Walls of a cell: bit d set when its neighbour in direction d (x+, x-, y+,
+// y-, z+, z-) is solid.
+__device__ __forceinline__ unsigned wall_bits(const SolidBits& s, int x, int y, int z) {
+    return (unsigned)cell_solid(s, x + 1, y, z) | (unsigned)cell_solid(s, x - 1, y, z) << 1 |
+           (unsigned)cell_solid(s, x, y + 1, z) << 2 | (unsigned)cell_solid(s, x, y - 1, z) << 3 |
+           (unsigned)cell_solid(s, x, y, z + 1) << 4 | (unsigned)cell_solid(s, x, y, z - 1) << 5;
+}
+
+// 1/2 for every axis among `axes_mask` (two bits per axis) that has a bit set.
+__device__ __forceinline__ double half_per_axis(unsigned m, int skip_axis) {
+    double w = 1.0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+        if (b != skip_axis && ((m >> (2 * b)) & 3u)) w *= 0.5;
+    return w;
+}
+
+// Discrete SLF energy between the two latest levels u1 (newest) and u0, in
+// FP64, over the air cells 1..n-2: 1/2 sum w_i (u1_i-u0_i)^2 + lambda2/2 sum
+// over edges between air cells of w_e (u1_i-u1_j)(u0_i-u0_j) (edges to the
+// fixed outer faces included once). A boundary cell's update mirrors its
+// neighbour across each wall, which makes it a half cell per walled axis:
+// w_i = 1/2 per axis with a wall, and an edge lying along walls takes 1/2
+// for each other axis on which both ends have the same wall. With walls of
+// frequency-independent admittance beta >= 0 around a convex air region the
+// energy changes by minus the wall loss each step (non-increasing; constant
+// for rigid walls); without a model every cell is air and every weight 1.
 template <typename T>
-__global__ void k_energy(const T* u1_, const T* u0_, float inv1, float inv0, GridDev g, double lambda2,
-                         double* out) {
+__global__ void k_energy(const T* u1_, const T* u0_, float inv1, float inv0, GridDev g, SolidBits sb,
+                         double lambda2, double* out) {
     auto u1 = [&](int64_t k) { return (double)fld(u1_ + k, inv1); };
     auto u0 = [&](int64_t k) { return (double)fld(u0_ + k, inv0); };
     const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int z = 1 + blockIdx.z;
     double acc = 0.0;
-    if (x <= g.nx - 2 && y <= g.ny - 2) {
+    if (x <= g.nx - 2 && y <= g.ny - 2 && !cell_solid(sb, x, y, z)) {
         const int64_t i = (int64_t)z * g.plane + (int64_t)y * g.pitch + x;
+        const unsigned mi = wall_bits(sb, x, y, z);
         const double d = u1(i) - u0(i);
-        acc = 0.5 * d * d;
+        acc = 0.5 * half_per_axis(mi, -1) * d * d;
         const int64_t off[3] = {1, g.pitch, g.plane};
-        const int lo[3] = {x, y, z};
+        const int c[3] = {x, y, z};
         double pot = 0.0;
         for (int ax = 0; ax < 3; ++ax) {
-            const int64_t jp = i + off[ax];
-            pot += (u1(i) - u1(jp)) * (u0(i) - u0(jp));
-            if (lo[ax] == 1) {
-                const int64_t jm = i - off[ax];
-                pot += (u1(i) - u1(jm)) * (u0(i) - u0(jm));
+            for (int sgn = 1; sgn >= -1; sgn -= 2) {
+                if (sgn < 0 && c[ax] != 1) break;  // the low edge only toward the outer face
+                int q[3] = {x, y, z};
+                q[ax] += sgn;
+                if (cell_solid(sb, q[0], q[1], q[2])) continue;
+                const int64_t j = i + sgn * off[ax];
+                const double we = half_per_axis(mi & wall_bits(sb, q[0], q[1], q[2]), ax);
+                pot += we * (u1(i) - u1(j)) * (u0(i) - u0(j));
             }
         }
         acc += 0.5 * lambda2 * pot;
@@ -2734,11 +2767,11 @@ double Engine::energy(int32_t batch) {
         const float inv1 = 1.0f / D.host_level_scale(batch, g), inv0 = 1.0f / D.host_level_scale(batch, g - 1);
         k_energy<__half><<<grd, blk, 0, D.stream>>>(h + (size_t)buf_new(g) * stride + base,
                                                     h + (size_t)buf_cur(g) * stride + base, inv1, inv0, gd,
-                                                    (double)D.lambda2(), D.d_energy.ptr);
+                                                    D.solid_view(), (double)D.lambda2(), D.d_energy.ptr);
     } else {
         k_energy<float><<<grd, blk, 0, D.stream>>>(D.fields.ptr + (size_t)buf_new(g) * stride + base,
                                                    D.fields.ptr + (size_t)buf_cur(g) * stride + base, 1.0f, 1.0f,
-                                                   gd, (double)D.lambda2(), D.d_energy.ptr);
+                                                   gd, D.solid_view(), (double)D.lambda2(), D.d_energy.ptr);
     }
     CK(cudaGetLastError());
     double e = 0.0;

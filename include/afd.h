@@ -275,7 +275,12 @@ typedef struct afd_info {
 int afd_get_info(afd_sim* s, afd_info* info);
 
 /* Discrete energy of the SLF scheme, accumulated in FP64 on the GPU:
- * kinetic + potential terms between the two latest time levels. */
+ * kinetic + potential terms between the two latest time levels, over the air
+ * cells 1..n-2 and the edges between air cells. A cell with walls (solid
+ * neighbours) counts 1/2 per walled axis, an edge 1/2 per other axis on which
+ * both ends have the same wall; without a model every weight is 1. Constant
+ * for rigid walls and non-increasing for passive walls (constant admittance
+ * >= 0) around a box-shaped room without PML. */
 int afd_energy(afd_sim* s, int32_t batch, double* energy);
 
 /* Runs the simulation's work on the caller's CUDA stream (a cudaStream_t

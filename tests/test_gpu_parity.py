@@ -188,3 +188,40 @@ def test_rigid_box_energy_conserved(pkg):
     e1 = sim.energy()
     assert e0 > 0
     assert abs(e1 - e0) / e0 < 1e-5
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_walled_box_energy(pkg, storage):
+    """FIXED scheme, box-shaped room in one-cell walls, no PML: the GPU's
+    FP64 energy equals the numpy restatement of the weighted energy on the
+    same two levels, is constant for rigid walls and never increases for
+    passive one-coefficient LRS walls."""
+    from test_energy_weights import PULSE, walled_box, weighted_energy
+    vox = walled_box(40, 32, 28)
+    solid = vox != -1
+    for a, rigid in ((np.zeros((3, 1), np.float32), True),
+                     (np.array([[0.15], [0.4], [0.25]], np.float32), False)):
+        sim = pkg.Simulation(mode=1, storage=storage)
+        sim.SetModel(pkg.Model.from_voxels(vox, a, np.ones((3, 1), np.float32)))
+        sim.AddSourceCell((12, 10, 9), PULSE)
+        sim.Run(40)
+        lam2 = float(sim.info().lambda2)
+        energies = []
+        for k in range(10):
+            f0 = sim.field()
+            sim.Run(1)
+            e = sim.energy()
+            if k in (0, 9):
+                want = weighted_energy(sim.field(), f0, solid, lam2)
+                assert abs(e - want) <= 1e-9 * want
+            energies.append(e)
+            sim.Run(39)
+        sim.close()
+        e = np.array(energies)
+        assert e[0] > 0
+        tol = 1e-6 if storage == 0 else 1e-2  # FP16 levels: storage rounding
+        if rigid:
+            assert np.ptp(e) / e[0] < tol
+        else:
+            assert np.all(e[1:] <= e[:-1] * (1 + tol))
+            assert e[-1] < 0.1 * e[0]
