@@ -1411,36 +1411,6 @@ struct Engine::Impl {
             CK(cudaStreamWaitEvent(stream, side_ev[k], 0));
         }
     }
-    // Work left running beside the main stream: each item on its own
-    // stream from the main stream's current point, joined back to the main
-    // stream by join_deferred() (or at the end of a captured chunk).
-    std::vector<cudaStream_t> def_side;
-    std::vector<cudaEvent_t> def_ev;
-    cudaEvent_t def_fork = nullptr;
-    size_t def_pending = 0;
-    void run_deferred(const std::vector<std::function<void(cudaStream_t)>>& work) {
-        if (work.empty()) return;
-        while (def_side.size() < work.size()) {
-            cudaStream_t st;
-            cudaEvent_t e;
-            CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-            def_side.push_back(st);
-            def_ev.push_back(e);
-        }
-        if (!def_fork) CK(cudaEventCreateWithFlags(&def_fork, cudaEventDisableTiming));
-        CK(cudaEventRecord(def_fork, stream));
-        for (size_t k = 0; k < work.size(); ++k) {
-            CK(cudaStreamWaitEvent(def_side[k], def_fork, 0));
-            work[k](def_side[k]);
-            CK(cudaEventRecord(def_ev[k], def_side[k]));
-        }
-        def_pending = work.size();
-    }
-    void join_deferred() {
-        for (size_t k = 0; k < def_pending; ++k) CK(cudaStreamWaitEvent(stream, def_ev[k], 0));
-        def_pending = 0;
-    }
     template <typename T>
     void launch_step_t(int j, bool profile);
     int64_t kernels_per_step() const;
@@ -2044,37 +2014,18 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         // disjoint cells and read only levels n and n-1 and the old
         // auxiliary fields, so they run side by side; the auxiliary updates
         // (one per axis, disjoint outputs) follow once both are done.
-        //
-        // FP32 storage with no source where the auxiliary updates read: the
-        // auxiliary updates of step n read levels n+1 and n, psi and the old
-        // auxiliary fields and write only the new auxiliary fields, none of
-        // which the next step's streaming kernel (reads n+1 and n, writes
-        // n+2) touches. They run beside the source/receiver kernel and the
-        // next streaming kernel, and the next PML pressure (which reads
-        // their output) waits for them.
         std::vector<std::function<void(cudaStream_t)>> g1, g2;
         if (a.lrs.n > 0) g1.push_back(lrs_launch);
         for (const PmlBox& bx : pml_boxes) g1.push_back([&, bx](cudaStream_t st) { pml_p_launch(bx, st); });
-        const bool defer = src_beside_aux && !f16();
-        for (int ax = 0; ax < 3; ++ax) {
-            if (defer) {
-                if (!pml_axis_boxes[ax].empty())
-                    g2.push_back([&, ax](cudaStream_t st) {
-                        for (const PmlBox& bx : pml_axis_boxes[ax]) pml_aux_launch(ax, bx, st);
-                    });
-            } else {
-                for (const PmlBox& bx : pml_axis_boxes[ax])
-                    g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
-            }
-        }
-        if (!defer && src_beside_aux && (a.src.n > 0 || a.rcv.n > 0)) {
+        for (int ax = 0; ax < 3; ++ax)
+            for (const PmlBox& bx : pml_axis_boxes[ax])
+                g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
+        if (src_beside_aux && (a.src.n > 0 || a.rcv.n > 0)) {
             g2.push_back([&](cudaStream_t st) { src_rcv_launch(st); });
             src_done = true;
         }
-        join_deferred();  // the auxiliary updates of the previous step
         run_side_by_side(g1);
-        if (defer) run_deferred(g2);
-        else run_side_by_side(g2);
+        run_side_by_side(g2);
     } else {
         if (a.lrs.n > 0) {
             begin(KK_LRS);
@@ -2130,7 +2081,6 @@ cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
     for (int64_t j = 0; j < n; ++j) launch_step((int)j, false);
-    join_deferred();  // before the step counter moves
     k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
     CK(cudaStreamEndCapture(stream, &graph));
     launches = saved;
@@ -2153,7 +2103,6 @@ void Engine::Impl::run_chunk(int64_t n) {
     } else {
         if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
         for (int64_t j = 0; j < n; ++j) launch_step((int)j, profile);
-        join_deferred();
         k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
         ++launches;
     }
@@ -2233,9 +2182,6 @@ Engine::~Engine() {
     for (auto st : D.side) cudaStreamDestroy(st);
     for (auto e : D.side_ev) cudaEventDestroy(e);
     if (D.fork_ev) cudaEventDestroy(D.fork_ev);
-    for (auto st : D.def_side) cudaStreamDestroy(st);
-    for (auto e : D.def_ev) cudaEventDestroy(e);
-    if (D.def_fork) cudaEventDestroy(D.def_fork);
     if (D.tev0) cudaEventDestroy(D.tev0);
     if (D.tev1) cudaEventDestroy(D.tev1);
     if (D.own_stream) cudaStreamDestroy(D.own_stream);
