@@ -64,7 +64,8 @@ class Info(C.Structure):
                 ("lambda2", C.c_float), ("mode", C.c_int32), ("storage", C.c_int32),
                 ("last_run_ms", C.c_double), ("kernel_launches", C.c_int64),
                 ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("tile_z", C.c_int32),
-                ("stream_blocks", C.c_int32), ("tuned", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("stream_blocks", C.c_int32), ("tuned", C.c_int32), ("stream_beside", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_int64, C.c_void_p)

@@ -2463,7 +2463,11 @@ int Engine::run(int64_t steps, afd_progress_fn cb, void* user) {
         // candidate plan, timed on the device; then the fastest is kept
         const bool measure = D.tune_active() && n == 200 && D.tune_next < D.tune_cands.size();
         if (measure) {
+            // the candidate's graph is captured, instantiated and uploaded
+            // before the clock starts: host work inside the timed region
+            // would leave the GPU idle and bias the choice
             D.apply_plan((int)D.tune_next + 1);
+            CK(cudaGraphUpload(D.graph_for(n), D.stream));
             CK(cudaEventRecord(D.tev0, D.stream));
         }
         D.run_chunk(n);
@@ -2733,6 +2737,7 @@ void Engine::get_info(afd_info* info) {
     info->tile_y = FT_Y;
     info->tile_z = D.fdev.dz;
     info->stream_blocks = D.fused_grid;
+    info->stream_beside = D.lists_beside() ? 1 : 0;
     info->tuned = D.tuned ? 1 : 0;
 }
 

@@ -528,7 +528,8 @@ def main():
     line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "plan": {"tile": [sim.info().tile_x, sim.info().tile_y, sim.info().tile_z],
-                     "stream_blocks": sim.info().stream_blocks, "tuned": bool(sim.info().tuned)},
+                     "stream_blocks": sim.info().stream_blocks, "beside": bool(sim.info().stream_beside),
+                     "tuned": bool(sim.info().tuned)},
             "dtype": "f32", "data": "synthetic", "config": config, "gpu_launches": launches, "clocks": clk}
     if "e2e" in legs:
         line["e2e"] = e2e_leg(sim, cfg, K, interior, world, metric)

@@ -270,7 +270,8 @@ typedef struct afd_info {
     int32_t tile_x, tile_y, tile_z;  /* tile (cells) and z-chunk depth of the streaming kernel's plan */
     int32_t stream_blocks;       /* resident blocks of the streaming kernel's plan */
     int32_t tuned;               /* 1 once the online autotuner has chosen the plan */
-    int32_t reserved[7];
+    int32_t stream_beside;       /* 1: the plan runs the boundary and PML kernels beside the streaming kernel */
+    int32_t reserved[6];
 } afd_info;
 int afd_get_info(afd_sim* s, afd_info* info);
 
