@@ -368,13 +368,16 @@ __device__ __forceinline__ bool box_cell(const PmlBox& bx, int& b, int& x, int& 
     return true;
 }
 
-__device__ __forceinline__ void row5(const float* p, float r[5]) {
+// Values x..x+4 of a row (x a multiple of 4). hi = false: the fifth value
+// is not needed (the unit's last cell is not updated) and not loaded; at the
+// end of a row it would cost a DRAM sector of the next row for one value.
+__device__ __forceinline__ void row5(const float* p, float r[5], bool hi = true) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(p));
     r[0] = v.x;
     r[1] = v.y;
     r[2] = v.z;
     r[3] = v.w;
-    r[4] = __ldg(p + 4);
+    r[4] = hi ? __ldg(p + 4) : 0.0f;
 }
 
 __device__ __forceinline__ void store4(float* p, const float v[4], unsigned m) {
@@ -390,10 +393,10 @@ __device__ __forceinline__ void store4(float* p, const float v[4], unsigned m) {
 // The same for a pressure level of either storage: FP16 rows decode with
 // 1/s (eight-byte loads of four values) and stores encode v * s.
 template <typename T>
-__device__ __forceinline__ void row5t(const T* p, float r[5], float inv) {
+__device__ __forceinline__ void row5t(const T* p, float r[5], float inv, bool fifth = true) {
     if constexpr (sizeof(T) == 4) {
         (void)inv;
-        row5(p, r);
+        row5(p, r, fifth);
     } else {
         const uint2 w = __ldg(reinterpret_cast<const uint2*>(p));
         const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
@@ -402,7 +405,7 @@ __device__ __forceinline__ void row5t(const T* p, float r[5], float inv) {
         r[1] = lo.y * inv;
         r[2] = hi.x * inv;
         r[3] = hi.y * inv;
-        r[4] = __half2float(__ldg(p + 4)) * inv;
+        r[4] = fifth ? __half2float(__ldg(p + 4)) * inv : 0.0f;
     }
 }
 
@@ -450,14 +453,16 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
         io = sc.inv_old;
     }
     const int lv = pml_level(a, g);
+    // x+4 is read only for the unit's last cell, x-1 only for its first
+    const bool hi = (m & 8u) != 0;
     float c[5], ym4[5], yp4[5], zm4[5], zp4[5], o[5];
-    row5t(pc + i, c, ic);
-    const float xm = fldg(pc + i - 1, ic);
-    row5t(pc + i - pitch, ym4, ic);
-    row5t(pc + i + pitch, yp4, ic);
-    row5t(pc + i - plane, zm4, ic);
-    row5t(pc + i + plane, zp4, ic);
-    row5t(po + i, o, io);
+    row5t(pc + i, c, ic, hi);
+    const float xm = (m & 1u) ? fldg(pc + i - 1, ic) : 0.0f;
+    row5t(pc + i - pitch, ym4, ic, false);
+    row5t(pc + i + pitch, yp4, ic, false);
+    row5t(pc + i - plane, zm4, ic, false);
+    row5t(pc + i + plane, zp4, ic, false);
+    row5t(po + i, o, io, false);
     const float4 kx4 = __ldg(reinterpret_cast<const float4*>(P.ksi[0] + x));
     const float kxv[4] = {kx4.x, kx4.y, kx4.z, kx4.w};
     const float ky = __ldg(P.ksi[1] + y), kz = __ldg(P.ksi[2] + z);
@@ -466,10 +471,10 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
     if (ra & 1u) {
         const float* f = P.fi[0][lv ^ 1] + base + i;
         float r00[5], r01[5], r10[5], r11[5], av[5];
-        row5(f, r00);
-        row5(f + plane, r01);
-        row5(f + pitch, r10);
-        row5(f + pitch + plane, r11);
+        row5(f, r00, hi);
+        row5(f + plane, r01, hi);
+        row5(f + pitch, r10, hi);
+        row5(f + pitch + plane, r11, hi);
 #pragma unroll
         for (int q = 0; q < 5; ++q) av[q] = 0.25f * (((r00[q] + r01[q]) + r10[q]) + r11[q]);
 #pragma unroll
@@ -478,10 +483,10 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
     if (ra & 2u) {
         const float* f = P.fi[1][lv ^ 1] + base + i;
         float r00[5], r01[5], r10[5], r11[5];
-        row5(f, r00);
-        row5(f + plane, r01);
-        row5(f + pitch, r10);
-        row5(f + pitch + plane, r11);
+        row5(f, r00, hi);
+        row5(f + plane, r01, hi);
+        row5(f + pitch, r10, hi);
+        row5(f + pitch + plane, r11, hi);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float a1 = 0.25f * (((r10[q] + r11[q]) + r10[q + 1]) + r11[q + 1]);
@@ -493,10 +498,10 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
     if (ra & 4u) {
         const float* f = P.fi[2][lv ^ 1] + base + i;
         float r00[5], r01[5], r10[5], r11[5];
-        row5(f, r00);
-        row5(f + plane, r01);
-        row5(f + pitch, r10);
-        row5(f + pitch + plane, r11);
+        row5(f, r00, hi);
+        row5(f + plane, r01, hi);
+        row5(f + pitch, r10, hi);
+        row5(f + pitch + plane, r11, hi);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float a1 = 0.25f * (((r01[q] + r11[q]) + r01[q + 1]) + r11[q + 1]);
@@ -578,25 +583,26 @@ __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ Ste
         ic = sc.inv_cur;
     }
     const int lv = pml_level(a, g);
+    const bool hi = (m & 8u) != 0;  // x+4 is read only for the unit's last cell
     float n00[5], n01[5], n10[5], n11[5], m00[5], m01[5], m10[5], m11[5];
-    row5t(pn, n00, in_);
-    row5t(pn + plane, n01, in_);
-    row5t(pn + pitch, n10, in_);
-    row5t(pn + pitch + plane, n11, in_);
-    row5t(pc, m00, ic);
-    row5t(pc + plane, m01, ic);
-    row5t(pc + pitch, m10, ic);
-    row5t(pc + pitch + plane, m11, ic);
+    row5t(pn, n00, in_, hi);
+    row5t(pn + plane, n01, in_, hi);
+    row5t(pn + pitch, n10, in_, hi);
+    row5t(pn + pitch + plane, n11, in_, hi);
+    row5t(pc, m00, ic, hi);
+    row5t(pc + plane, m01, ic, hi);
+    row5t(pc + pitch, m10, ic, hi);
+    row5t(pc + pitch + plane, m11, ic, hi);
     float s00[5] = {0}, s01[5] = {0}, s10[5] = {0}, s11[5] = {0};
     if (PSI) {
         const float* ps = P.psi[lv] + base + i;
-        row5(ps, s00);
-        row5(ps + plane, s01);
-        row5(ps + pitch, s10);
-        row5(ps + pitch + plane, s11);
+        row5(ps, s00, hi);
+        row5(ps + plane, s01, hi);
+        row5(ps + pitch, s10, hi);
+        row5(ps + pitch + plane, s11, hi);
     }
     float kxs[5];
-    row5(P.ksi[0] + x, kxs);
+    row5(P.ksi[0] + x, kxs, hi);
     const float kay = 0.5f * (__ldg(P.ksi[1] + y) + __ldg(P.ksi[1] + y + 1));
     const float kaz = 0.5f * (__ldg(P.ksi[2] + z) + __ldg(P.ksi[2] + z + 1));
     const float4 f14 = *reinterpret_cast<const float4*>(P.fi[AX][lv ^ 1] + base + i);
