@@ -129,20 +129,28 @@ __host__ __device__ inline int max_slot(long long L) { return (int)(((L % 5) + 5
 // m' = max(m, smax) < 2^e (frexp's exponent), 1 when m' is 0, exponent
 // clamped to [-60, 60]. The 2^6 headroom below the binary16 maximum covers
 // the growth of two steps.
-__host__ __device__ inline float level_scale(uint32_t mbits, float smax) {
+__host__ __device__ inline int level_scale_exp(uint32_t mbits, float smax) {
     float m;
     memcpy(&m, &mbits, 4);
     const float a = m > smax ? m : smax;
-    if (!(a > 0.0f)) return 1.0f;
+    if (!(a > 0.0f)) return 0;
     uint32_t ab;
     memcpy(&ab, &a, 4);
     const int e = (int)((ab >> 23) & 0xffu) - 126;  // frexp exponent of a normal a
-    int k = 10 - e;
-    k = k > 60 ? 60 : (k < -60 ? -60 : k);
+    const int k = 10 - e;
+    return k > 60 ? 60 : (k < -60 ? -60 : k);
+}
+
+// 2^k for |k| <= 60 (a normal float, built from its exponent bits).
+__host__ __device__ inline float pow2_exact(int k) {
     const uint32_t sb = (uint32_t)(k + 127) << 23;
-    float sc;
-    memcpy(&sc, &sb, 4);
-    return sc;
+    float v;
+    memcpy(&v, &sb, 4);
+    return v;
+}
+
+__host__ __device__ inline float level_scale(uint32_t mbits, float smax) {
+    return pow2_exact(level_scale_exp(mbits, smax));
 }
 
 // Scales of the levels step g reads and writes for member b.
@@ -152,16 +160,24 @@ struct StepScales {
     float s_old, inv_old;  // level g - 2 (p^{n-1})
 };
 
+// The slots read here (levels g-2..g-4) are written only by the interior
+// kernels of earlier steps (step g writes slot g-1 and clears slot g), so
+// they are read through the read-only cache: one L2 request per SM instead
+// of one per warp at the same address. 1/s is 2^-k exactly (what 1.0f / s
+// gives for a power of two).
 __device__ __forceinline__ StepScales step_scales(const F16Dev& f, int b, long long g) {
     const uint32_t* mx = f.mx + (size_t)b * 5;
     const float smax = __ldg(f.src_max + b);
+    const int kn = level_scale_exp(__ldg(mx + max_slot(g - 2)), smax);
+    const int kc = level_scale_exp(__ldg(mx + max_slot(g - 3)), smax);
+    const int ko = level_scale_exp(__ldg(mx + max_slot(g - 4)), smax);
     StepScales s;
-    s.s_new = level_scale(*(volatile const uint32_t*)(mx + max_slot(g - 2)), smax);
-    s.s_cur = level_scale(*(volatile const uint32_t*)(mx + max_slot(g - 3)), smax);
-    s.s_old = level_scale(*(volatile const uint32_t*)(mx + max_slot(g - 4)), smax);
-    s.inv_new = 1.0f / s.s_new;
-    s.inv_cur = 1.0f / s.s_cur;
-    s.inv_old = 1.0f / s.s_old;
+    s.s_new = pow2_exact(kn);
+    s.s_cur = pow2_exact(kc);
+    s.s_old = pow2_exact(ko);
+    s.inv_new = pow2_exact(-kn);
+    s.inv_cur = pow2_exact(-kc);
+    s.inv_old = pow2_exact(-ko);
     return s;
 }
 
