@@ -38,6 +38,7 @@ EXPORTS = [
     "afd_set_pml_profile", "afd_add_source", "afd_add_source_cell", "afd_add_receiver",
     "afd_add_receiver_cell", "afd_run", "afd_prepare", "afd_get_receivers", "afd_update_source",
     "afd_get_receivers_range", "afd_get_field", "afd_get_plane", "afd_set_capture", "afd_get_frames",
+    "afd_set_timeline", "afd_get_timeline",
     "afd_get_info", "afd_energy", "afd_set_stream", "afd_kernel_stats", "afd_last_error",
     "afd_destroy",
 ]
@@ -120,6 +121,8 @@ def library(path=LIB_PATH):
         "afd_get_plane": (C.c_int, [vp, i32, i32, i32, P(f32), i64]),
         "afd_set_capture": (C.c_int, [vp, i32, i32, i32, i32, i32]),
         "afd_get_frames": (C.c_int, [vp, P(f32), i64, P(i64), i64, P(i32)]),
+        "afd_set_timeline": (C.c_int, [vp, i64, i32]),
+        "afd_get_timeline": (C.c_int, [vp, P(f64), i64, P(i32)]),
         "afd_get_info": (C.c_int, [vp, P(Info)]),
         "afd_energy": (C.c_int, [vp, i32, P(f64)]),
         "afd_set_stream": (C.c_int, [vp, vp]),
@@ -396,6 +399,27 @@ class Simulation:
         self._check(library().afd_get_frames(self._h, _ptr(out, C.c_float), out.size, _ptr(steps, C.c_int64),
                                              steps.size, C.byref(n)))
         return out[:n.value], steps[:n.value]
+
+    TIMELINE_KINDS = ("interior_stream", "boundary", "pml_pressure", "pml_aux_x", "pml_aux_y", "pml_aux_z",
+                      "source_receiver")
+
+    def set_timeline(self, first, steps):
+        """From the next Run on, record the start of the first block and the
+        end of the last block of every kernel kind of global steps
+        first .. first+steps-1 (device clock)."""
+        self._check(library().afd_set_timeline(self._h, first, steps))
+        self._tl_steps = max(int(steps), 0)
+
+    def timeline(self):
+        """[steps, len(TIMELINE_KINDS), 2] (start, end) in microseconds from
+        the earliest recorded start; NaN where a kind did not run."""
+        n_max = getattr(self, "_tl_steps", 0)
+        out = np.empty((max(n_max, 1), len(self.TIMELINE_KINDS), 2), np.float64)
+        n = C.c_int32()
+        self._check(library().afd_get_timeline(self._h, _ptr(out, C.c_double), out.size, C.byref(n)))
+        t = out[:n.value] / 1e3
+        t[out[:n.value] < 0] = np.nan
+        return t
 
     def energy(self, batch=0):
         e = C.c_double()

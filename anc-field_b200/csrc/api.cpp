@@ -335,6 +335,17 @@ int afd_set_capture(afd_sim* s, int32_t batch, int32_t axis, int32_t index, int3
     SIM_CALL(s, { s->eng->set_capture(batch, axis, index, every, max_frames); });
 }
 
+int afd_set_timeline(afd_sim* s, int64_t first, int32_t steps) {
+    SIM_CALL(s, { s->eng->set_timeline(first, steps); });
+}
+
+int afd_get_timeline(afd_sim* s, double* out, int64_t cap, int32_t* n_steps) {
+    SIM_CALL(s, {
+        const int32_t n = s->eng->get_timeline(out, cap);
+        if (n_steps) *n_steps = n;
+    });
+}
+
 int afd_get_frames(afd_sim* s, float* out, int64_t cap, int64_t* steps, int64_t steps_cap, int32_t* n_frames) {
     SIM_CALL(s, {
         const int32_t n = s->eng->get_frames(out, cap, steps, steps_cap);

@@ -108,6 +108,41 @@ struct StepArgs {
     SrcDev src;
     RcvDev rcv;
     int* flag;                // watchdog flag (bit0: |p| left the bound)
+    // step timeline (off when tl_start is null): for global steps
+    // tl_g0 .. tl_g0 + tl_steps - 1 and each of TL_SLOTS kernel kinds, the
+    // start of the first and the end of the last recording block (%globaltimer)
+    unsigned long long* tl_start;
+    unsigned long long* tl_end;
+    long long tl_g0;
+    int32_t tl_steps;
+};
+
+// Timeline slots: streaming or interior kernel, boundary, PML pressure,
+// PML auxiliary x, y, z, source/receiver.
+constexpr int TL_SLOTS = 7;
+
+// Marks one block of a kernel in the step timeline: thread 0 of a recording
+// block takes the start at construction and the end when it leaves the
+// kernel (every return path). `rec`: the block belongs to batch member 0
+// (the kernels with one block column per member) or to every member.
+struct TlMark {
+    unsigned long long* end = nullptr;
+    __device__ __forceinline__ static unsigned long long now() {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    }
+    __device__ __forceinline__ TlMark(const StepArgs& a, int slot, long long g, bool rec) {
+        if (!a.tl_start || !rec || (threadIdx.x | threadIdx.y | threadIdx.z)) return;
+        const long long d = g - a.tl_g0;
+        if (d < 0 || d >= a.tl_steps) return;
+        const size_t k = (size_t)d * TL_SLOTS + slot;
+        atomicMin(a.tl_start + k, now());
+        end = a.tl_end + k;
+    }
+    __device__ __forceinline__ ~TlMark() {
+        if (end) atomicMax(end, now());
+    }
 };
 
 // Buffer roles of global step g, following the pointer rotation of

@@ -75,6 +75,7 @@ __device__ __forceinline__ void watch(int* flag, float v) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 0, g, blockIdx.z < (unsigned)(a.g.nz - 2));
     const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int zn = a.g.nz - 2;
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
 template <bool REF, int KT, typename T>
 __global__ void __launch_bounds__(256, 5) k_lrs(const __grid_constant__ StepArgs a, int j) {
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 1, g, blockIdx.y == 0);
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.lrs.n) return;
     const int b = blockIdx.y;
@@ -281,6 +283,7 @@ __device__ __forceinline__ int pml_level(const StepArgs& a, long long g) {
 // new pressure and psi recomputed locally (nothing written that is read).
 __global__ void __launch_bounds__(256) k_pml_ref_aux(StepArgs a, int j) {
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 3, g, blockIdx.z < (unsigned)(a.g.nz - 4));
     const int x = 2 + blockIdx.x * blockDim.x + threadIdx.x;
     const int y = 2 + blockIdx.y * blockDim.y + threadIdx.y;
     const int zn = a.g.nz - 4;
@@ -313,6 +316,7 @@ __global__ void __launch_bounds__(256) k_pml_ref_aux(StepArgs a, int j) {
 // REF pass 2: pressure and psi of every cell 2..n-3 (pml.cl:182-207).
 __global__ void __launch_bounds__(256) k_pml_ref_p(StepArgs a, int j) {
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 2, g, blockIdx.z < (unsigned)(a.g.nz - 4));
     const int x = 2 + blockIdx.x * blockDim.x + threadIdx.x;
     const int y = 2 + blockIdx.y * blockDim.y + threadIdx.y;
     const int zn = a.g.nz - 4;
@@ -439,6 +443,7 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
     if (!m) return;
     const PmlDev& P = a.pml;
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 2, g, blockIdx.z < (unsigned)bx.depth);
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
     const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
@@ -565,6 +570,7 @@ __global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepA
 template <int AX, bool PSI, typename T>
 __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ StepArgs a, const PmlBox bx,
                                                      int j) {
+    const TlMark tl(a, 3 + AX, *a.d_step + j, blockIdx.z < (unsigned)bx.depth);
     int b, x, y, z;
     if (!box_cell(bx, b, x, y, z)) return;
     const unsigned m = pml_mask4(a, x, y, z);
@@ -680,6 +686,7 @@ template <typename T>
 __global__ void __launch_bounds__(F_THREADS, 2)
     k_stream(const __grid_constant__ CUtensorMap tm_halo, const __grid_constant__ CUtensorMap tm_own,
              const __grid_constant__ StepArgs a, const __grid_constant__ FusedDev f, int j) {
+    const TlMark tl(a, 0, *a.d_step + j, true);
     using TL = Tile<T>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
@@ -963,6 +970,7 @@ __device__ __forceinline__ float2 new_level_scale(const StepArgs& a, int b, long
 template <typename T>
 __global__ void k_src_rcv(StepArgs a, int j, int do_src, int do_rcv) {
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 6, g, blockIdx.x == 0);
     const int b = blockIdx.x;
     T* pn = level_ptr<T>(a, buf_new(g)) + (size_t)b * a.g.vol;
     const float2 sc = new_level_scale<T>(a, b, g);
@@ -999,6 +1007,7 @@ template <typename T>
 __global__ void k_src_rcv_inline(const __grid_constant__ StepArgs a, const __grid_constant__ SrcRcvInline q,
                                  int j) {
     const long long g = *a.d_step + j;
+    const TlMark tl(a, 6, g, blockIdx.x == 0);
     const int b = blockIdx.x;
     T* pn = level_ptr<T>(a, buf_new(g)) + (size_t)b * a.g.vol;
     const float2 sc = new_level_scale<T>(a, b, g);
@@ -1208,6 +1217,11 @@ struct Engine::Impl {
     int64_t cap_total = 0;  // frames captured so far
     DBuf<float> cap_frames;
     DBuf<long long> cap_steps, cap_run0;
+    // step timeline (afd_set_timeline)
+    DBuf<unsigned long long> tl_start, tl_end;
+    long long tl_first = 0;
+    int32_t tl_steps = 0;
+    bool tl_dirty = false;
     CaptureDev cap{};
     void advance_done(int64_t n) {
         if (cap_every > 0 && n > 0) cap_total += (n + cap_every - 1) / cap_every;
@@ -1880,6 +1894,10 @@ void Engine::Impl::build_args() {
     a.rcv.out = rcv_out.ptr;
     a.rcv.cap = rcv_cap;
     a.flag = d_flag.ptr;
+    a.tl_start = tl_steps > 0 ? tl_start.ptr : nullptr;
+    a.tl_end = tl_steps > 0 ? tl_end.ptr : nullptr;
+    a.tl_g0 = tl_first;
+    a.tl_steps = tl_steps;
     // inline source/receiver table (device order of upload_sources)
     inline_ok = (int64_t)sources.size() <= kInlineSrc && (int64_t)receivers.size() <= kInlineRcv;
     inl = SrcRcvInline{};
@@ -2403,6 +2421,17 @@ void Engine::Impl::setup_run(int64_t steps) {
         cap_dirty = false;
         drop_graphs();
     }
+    if (tl_dirty) {
+        if (tl_steps > 0) {
+            const size_t n = (size_t)tl_steps * TL_SLOTS;
+            tl_start.alloc(n);
+            tl_end.alloc(n);
+            CK(cudaMemsetAsync(tl_start.ptr, 0xff, n * sizeof(unsigned long long), stream));
+            CK(cudaMemsetAsync(tl_end.ptr, 0, n * sizeof(unsigned long long), stream));
+        }
+        tl_dirty = false;
+        drop_graphs();  // the kernels' arguments carry the timeline buffers
+    }
     if (cap_every > 0) {
         const long long r0[2] = {(long long)steps_done, (long long)cap_total};
         CK(cudaMemcpyAsync(cap_run0.ptr, r0, sizeof(r0), cudaMemcpyHostToDevice, stream));
@@ -2662,6 +2691,36 @@ void Engine::set_capture(int32_t batch, int32_t axis, int32_t index, int32_t eve
     D.cap_every = every > 0 ? every : 0;
     D.cap_max = every > 0 ? max_frames : 0;
     D.cap_dirty = true;
+}
+
+void Engine::set_timeline(int64_t first, int32_t steps) {
+    Impl& D = *d_;
+    if (steps > 4096) throw Error(AFD_ERR_ARG, "timeline steps must be at most 4096");
+    if (first < 0) throw Error(AFD_ERR_ARG, "first step must be >= 0");
+    D.tl_first = first;
+    D.tl_steps = steps > 0 ? steps : 0;
+    D.tl_dirty = true;
+}
+
+int32_t Engine::get_timeline(double* out, int64_t cap) {
+    Impl& D = *d_;
+    if (D.tl_steps <= 0 || D.tl_dirty || !D.tl_start.ptr) return 0;
+    const size_t n = (size_t)D.tl_steps * TL_SLOTS;
+    if (out && cap < (int64_t)(2 * n)) throw Error(AFD_ERR_ARG, "output buffer too small: need " + std::to_string(2 * n));
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamSynchronize(D.stream));
+    std::vector<unsigned long long> st(n), en(n);
+    CK(cudaMemcpy(st.data(), D.tl_start.ptr, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(en.data(), D.tl_end.ptr, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    unsigned long long t0 = ~0ull;
+    for (size_t k = 0; k < n; ++k) t0 = std::min(t0, st[k]);
+    if (out)
+        for (size_t k = 0; k < n; ++k) {
+            const bool ok = st[k] != ~0ull && en[k] >= st[k];
+            out[2 * k] = ok ? (double)(st[k] - t0) : -1.0;
+            out[2 * k + 1] = ok ? (double)(en[k] - t0) : -1.0;
+        }
+    return D.tl_steps;
 }
 
 int32_t Engine::get_frames(float* out, int64_t cap, int64_t* steps, int64_t steps_cap) {

@@ -42,6 +42,8 @@ public:
     void get_plane(int32_t batch, int32_t axis, int32_t index, float* out, int64_t cap);
     void set_capture(int32_t batch, int32_t axis, int32_t index, int32_t every, int32_t max_frames);
     int32_t get_frames(float* out, int64_t cap, int64_t* steps, int64_t steps_cap);
+    void set_timeline(int64_t first, int32_t steps);
+    int32_t get_timeline(double* out, int64_t cap);
     void get_info(afd_info* info);
     double energy(int32_t batch);
     void set_stream(void* stream);

@@ -8,6 +8,8 @@ One step = one time step of the whole grid. Prints one JSON line.
           than L2, so no flush is needed between steps)
   e2e   : the same through the public API with the step's source samples
           copied host->device and the receiver samples device->host
+  timeline_us: per-kernel start/end inside the replayed step (device clock,
+          median over 32 steps after the timed runs)
   roofline: the step kernel's algorithmic bytes / its CUDA-event duration
   cpu_baseline: the reference's own kernels (oracle/_ref) on host cores
 
@@ -39,7 +41,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None,
                     help="NX,NY,NZ: the same construction at another size (profiling captures)")
-    ap.add_argument("--legs", default="device,e2e,roofline,cpu",
+    ap.add_argument("--legs", default="device,e2e,timeline,roofline,cpu",
                     help="comma list of device,e2e,roofline,cpu")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c3rooms", "c5", "lms", "gemm"],
                     help="c2: the single-source throughput line (default); c3: batched secondary-path IRs/s; "
@@ -451,7 +453,8 @@ def main():
     dims = tuple(int(v) for v in args.grid.split(",")) if args.grid else (512, 384, 320)
     # the source covers warm-up, the device leg and the e2e leg, so the e2e
     # leg's per-chunk source updates land in place
-    cfg = W.config_c2(steps=max(args.warmup, 3) + 2 * max(args.steps, 1) + 8 * 1001 + 400, dims=dims)
+    cfg = W.config_c2(steps=max(args.warmup, 3) + 2 * max(args.steps, 1) + 8 * 1001 + 400 + TIMELINE_RUN,
+                      dims=dims)
     nx, ny, nz = cfg.dims
     interior = (nx - 2) * (ny - 2) * (nz - 2)
     metric = "Mcell-updates/s"
@@ -533,6 +536,8 @@ def main():
             "dtype": "f32", "data": "synthetic", "config": config, "gpu_launches": launches, "clocks": clk}
     if "e2e" in legs:
         line["e2e"] = e2e_leg(sim, cfg, K, interior, world, metric)
+    if "timeline" in legs:
+        line["timeline_us"] = timeline_leg(sim)
     sim.close()
     if "roofline" in legs:
         line["roofline"] = roofline_leg(make_sim, K, interior, 6.0 if f16 else 12.0,
@@ -543,6 +548,30 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+TIMELINE_RUN = 240  # steps of the timeline leg (32 recorded)
+
+
+def timeline_leg(sim):
+    """Per-kernel device timeline of 32 steps after the timed runs (same
+    plan): median start and end of every kernel kind relative to its step's
+    streaming-kernel start, and the median step period, in microseconds."""
+    g0 = sim.info().steps_done + 100
+    sim.set_timeline(g0, 32)
+    sim.prepare(TIMELINE_RUN)
+    sim.Run(TIMELINE_RUN)
+    t = sim.timeline()
+    sim.set_timeline(0, 0)
+    if t.shape[0] == 0:
+        return None
+    base = t[:, 0, 0]
+    out = {"step": round(float(np.median(np.diff(base))), 2)}
+    for k, name in enumerate(sim.TIMELINE_KINDS):
+        if np.all(np.isnan(t[:, k, 0])):
+            continue
+        out[name] = [round(float(np.nanmedian(t[:, k, 0] - base)), 2), round(float(np.nanmedian(t[:, k, 1] - base)), 2)]
+    return out
 
 
 def e2e_leg(sim, cfg, K, interior, world, metric):

@@ -254,6 +254,22 @@ int afd_set_capture(afd_sim* s, int32_t batch, int32_t axis, int32_t index, int3
 int afd_get_frames(afd_sim* s, float* out, int64_t cap, int64_t* steps, int64_t steps_cap,
                    int32_t* n_frames);
 
+/* Step timeline (measurement, no reference counterpart): from the next run
+ * on, the kernels of global steps first .. first+steps-1 record on the
+ * device (%globaltimer) the start of their first block and the end of their
+ * last block, for AFD_TIMELINE_SLOTS kernel kinds: 0 streaming or interior
+ * kernel, 1 boundary (LRS) kernel, 2 PML pressure, 3/4/5 PML auxiliary
+ * update of fi_x/fi_y/fi_z, 6 source/receiver kernel. Kernels with one block
+ * column per batch member record member 0's blocks. steps <= 0 turns it
+ * off; at most 4096 steps. */
+#define AFD_TIMELINE_SLOTS 7
+int afd_set_timeline(afd_sim* s, int64_t first, int32_t steps);
+/* The recorded timeline: out[steps][AFD_TIMELINE_SLOTS][2] (start, end) in
+ * nanoseconds from the earliest recorded start, -1 where a kind did not run
+ * at a step; cap >= 2 * steps * AFD_TIMELINE_SLOTS; *n_steps receives the
+ * number of steps (0 when no timeline is armed). */
+int afd_get_timeline(afd_sim* s, double* out, int64_t cap, int32_t* n_steps);
+
 typedef struct afd_info {
     int32_t nx, ny, nz;          /* simulation grid */
     int32_t ncoef, nmat;
