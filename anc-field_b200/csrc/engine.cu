@@ -434,9 +434,11 @@ __device__ __forceinline__ void store4t(T* p, const float v[4], unsigned m, floa
 // Pressure of the PML cells (pml.cl:185-207 restricted to the slab cells)
 // over one box of the disjoint box cover, four consecutive cells per
 // thread. Fields outside the read axes are identically zero there and are
-// not loaded; PSI: psi is kept (PML faces on all three axes).
+// not loaded; PSI: psi is kept (PML faces on all three axes). Four blocks
+// per SM (64 registers, no spills in any variant): the FP16 build would
+// otherwise take 79 registers and three blocks.
 template <bool PSI, typename T>
-__global__ void __launch_bounds__(256) k_pml_box_p(const __grid_constant__ StepArgs a, const PmlBox bx, int j) {
+__global__ void __launch_bounds__(256, 4) k_pml_box_p(const __grid_constant__ StepArgs a, const PmlBox bx, int j) {
     int b, x, y, z;
     if (!box_cell(bx, b, x, y, z)) return;
     const unsigned m = pml_mask4(a, x, y, z);
