@@ -38,7 +38,7 @@ EXPORTS = [
     "afd_set_pml_profile", "afd_add_source", "afd_add_source_cell", "afd_add_receiver",
     "afd_add_receiver_cell", "afd_run", "afd_prepare", "afd_get_receivers", "afd_update_source",
     "afd_get_receivers_range", "afd_get_field", "afd_get_plane", "afd_set_capture", "afd_get_frames",
-    "afd_set_timeline", "afd_get_timeline",
+    "afd_set_timeline", "afd_get_timeline", "afd_wait_selftest",
     "afd_get_info", "afd_energy", "afd_set_stream", "afd_kernel_stats", "afd_last_error",
     "afd_destroy",
 ]
@@ -122,6 +122,7 @@ def library(path=LIB_PATH):
         "afd_set_capture": (C.c_int, [vp, i32, i32, i32, i32, i32]),
         "afd_get_frames": (C.c_int, [vp, P(f32), i64, P(i64), i64, P(i32)]),
         "afd_set_timeline": (C.c_int, [vp, i64, i32]),
+        "afd_wait_selftest": (C.c_int, [i32, i32, i32, P(i32), P(i64)]),
         "afd_get_timeline": (C.c_int, [vp, P(f64), i64, P(i32)]),
         "afd_get_info": (C.c_int, [vp, P(Info)]),
         "afd_energy": (C.c_int, [vp, i32, P(f64)]),
@@ -251,6 +252,16 @@ class Model:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.afd_model_destroy(self._h)
             self._h = None
+
+
+def wait_selftest(which, complete, device=0):
+    """Bounded-wait self-test on the GPU: (gave up, seconds waited) for
+    the streaming kernel's wait (which=0) or the GEMM kernels' (which=1)."""
+    t, ns = C.c_int32(), C.c_int64()
+    s = library().afd_wait_selftest(device, which, 1 if complete else 0, C.byref(t), C.byref(ns))
+    if s != OK:
+        raise AfdError(s, "wait self-test failed")
+    return bool(t.value), ns.value / 1e9
 
 
 def check_filters(a, b, n_freq=4096):

@@ -24,7 +24,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--expt-relaxed-c
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-I" + INC] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-I" + INC]
 
-CU_SOURCES = ["engine.cu", "filters.cu", "mlp.cu", "lms.cu", "geometry.cu"]
+CU_SOURCES = ["engine.cu", "filters.cu", "mlp.cu", "lms.cu", "geometry.cu", "selftest.cu"]
 CXX_SOURCES = ["model.cpp", "api.cpp"]
 HEADERS = ["device.cuh", "engine.hpp", "model.hpp", "filters.hpp", "fused.cuh", "tc.cuh", "geometry.hpp"]
 

@@ -311,6 +311,16 @@ int afd_set_stream(afd_sim* s, void* stream);
 int afd_kernel_stats(afd_sim* s, int32_t idx, char* name, int64_t cap,
                      int64_t* launches, double* ms);
 
+/* Self-test of the bounded device waits (no reference counterpart): one
+ * block on `device` waits on a shared-memory mbarrier with the streaming
+ * kernel's wait (which = 0) or the tensor-core GEMM kernels' wait
+ * (which = 1). complete = 0 leaves the barrier incomplete, so the wait gives
+ * up at its 2 s limit instead of hanging; *timed_out receives 1 when it gave
+ * up, *waited_ns the device time it waited. The kernel returns normally
+ * either way and the context stays usable. */
+int afd_wait_selftest(int32_t device, int32_t which, int32_t complete, int32_t* timed_out,
+                      int64_t* waited_ns);
+
 const char* afd_last_error(const afd_sim* s);
 void afd_destroy(afd_sim* s);
 
