@@ -2042,13 +2042,15 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         std::vector<std::function<void(cudaStream_t)>> g1, g2;
         if (a.lrs.n > 0) g1.push_back(lrs_launch);
         for (const PmlBox& bx : pml_boxes) g1.push_back([&, bx](cudaStream_t st) { pml_p_launch(bx, st); });
-        for (int ax = 0; ax < 3; ++ax)
-            for (const PmlBox& bx : pml_axis_boxes[ax])
-                g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
         if (src_beside_aux && (a.src.n > 0 || a.rcv.n > 0)) {
+            // queued first: its one block then starts at once instead of
+            // waiting for the auxiliary updates' blocks to be dispatched
             g2.push_back([&](cudaStream_t st) { src_rcv_launch(st); });
             src_done = true;
         }
+        for (int ax = 0; ax < 3; ++ax)
+            for (const PmlBox& bx : pml_axis_boxes[ax])
+                g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
         run_side_by_side(g1);
         run_side_by_side(g2);
     } else {
