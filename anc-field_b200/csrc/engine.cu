@@ -1276,7 +1276,7 @@ struct Engine::Impl {
         build_fused();
     }
     // candidates: the streaming kernel alone with all resident blocks per SM
-    // and z-chunk depth {rule, rule / 2}, or (FP32 storage) beside the
+    // and z-chunk depth {rule, rule / 2, rule / 4}, or (FP32 storage) beside the
     // boundary and PML kernels with {all, all - 1} blocks per SM; every
     // candidate gives the results of the serial order
     // candidates of the current model and grid, made once (the plan then
@@ -1297,6 +1297,7 @@ struct Engine::Impl {
         };
         add(max_per_sm, rule_dz, false);
         add(max_per_sm, rule_dz / 2, false);
+        add(max_per_sm, rule_dz / 4, false);
         // the plans with the boundary and PML kernels beside the streaming
         // kernel are offered for FP32 storage only: with FP16 storage they
         // gave results that differed from the serial order and between runs
