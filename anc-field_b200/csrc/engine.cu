@@ -2125,9 +2125,7 @@ void Engine::Impl::run_chunk(int64_t n) {
         cudaGraphExec_t g = graph_for(n);
         CK(cudaGraphLaunch(g, stream));
         // the graph holds n steps of kernels plus the step-counter advance
-        const int64_t before = launches;
         launch_step_count_only(n);
-        (void)before;
     } else {
         if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
         for (int64_t j = 0; j < n; ++j) launch_step((int)j, profile);
