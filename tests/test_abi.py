@@ -286,3 +286,37 @@ def test_device_kerkythea_loader_reports_missing_device_or_bad_file(pkg, tmp_pat
     with pytest.raises(pkg.AfdError) as ei:
         pkg.Model.load_kerkythea(str(tmp_path / "model.xml"), 0.02, device=0)
     assert ei.value.status == pkg.afd.ERR_CUDA
+
+
+def test_ctypes_structs_match_the_header(pkg, tmp_path):
+    """sizeof and every field offset of afd_params and afd_info as the C
+    compiler lays them out from include/afd.h, against the ctypes mirrors."""
+    import ctypes as C
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"afd_params": pkg.afd.Params, "afd_info": pkg.afd.Info}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "afd.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))
+        for fname, _ in py._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, fname, cname, fname))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {(a, b): int(c) for a, b, c in (line.split() for line in out if line)}
+    for cname, py in structs.items():
+        assert got[(cname, "sizeof")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_timeline_slots_match_the_header(pkg):
+    text = open(HEADER).read()
+    m = re.search(r"#define\s+AFD_TIMELINE_SLOTS\s+(\d+)", text)
+    assert m and int(m.group(1)) == len(pkg.Simulation.TIMELINE_KINDS)
