@@ -291,7 +291,6 @@ def test_device_kerkythea_loader_reports_missing_device_or_bad_file(pkg, tmp_pat
 def test_ctypes_structs_match_the_header(pkg, tmp_path):
     """sizeof and every field offset of afd_params and afd_info as the C
     compiler lays them out from include/afd.h, against the ctypes mirrors."""
-    import ctypes as C
     import shutil
     import subprocess
     cc = shutil.which("gcc") or shutil.which("cc")
