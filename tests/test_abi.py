@@ -289,15 +289,17 @@ def test_device_kerkythea_loader_reports_missing_device_or_bad_file(pkg, tmp_pat
 
 
 def test_ctypes_structs_match_the_header(pkg, tmp_path):
-    """sizeof and every field offset of afd_params and afd_info as the C
-    compiler lays them out from include/afd.h, against the ctypes mirrors."""
+    """sizeof and every field offset of afd_params, afd_info and
+    afd_mlp_params as the C compiler lays them out from include/, against
+    the ctypes mirrors."""
     import shutil
     import subprocess
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
-    structs = {"afd_params": pkg.afd.Params, "afd_info": pkg.afd.Info}
-    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "afd.h"', "int main(void) {"]
+    structs = {"afd_params": pkg.afd.Params, "afd_info": pkg.afd.Info, "afd_mlp_params": pkg.surrogate.MlpParams}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "afd.h"', '#include "afd_surrogate.h"',
+             "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))
         for fname, _ in py._fields_:
