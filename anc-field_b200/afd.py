@@ -39,7 +39,7 @@ EXPORTS = [
     "afd_add_receiver_cell", "afd_run", "afd_prepare", "afd_get_receivers", "afd_update_source",
     "afd_get_receivers_range", "afd_get_field", "afd_get_plane", "afd_set_capture", "afd_get_frames",
     "afd_set_timeline", "afd_get_timeline", "afd_wait_selftest",
-    "afd_get_info", "afd_energy", "afd_set_stream", "afd_kernel_stats", "afd_last_error",
+    "afd_get_info", "afd_energy", "afd_set_stream", "afd_set_plan", "afd_kernel_stats", "afd_last_error",
     "afd_destroy",
 ]
 
@@ -66,7 +66,12 @@ class Info(C.Structure):
                 ("last_run_ms", C.c_double), ("kernel_launches", C.c_int64),
                 ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("tile_z", C.c_int32),
                 ("stream_blocks", C.c_int32), ("tuned", C.c_int32), ("stream_beside", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("stream_per_sm", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
+class Plan(C.Structure):
+    _fields_ = [("tile_x", C.c_int32), ("tile_y", C.c_int32), ("per_sm", C.c_int32), ("dz", C.c_int32),
+                ("beside", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_int64, C.c_void_p)
@@ -127,6 +132,7 @@ def library(path=LIB_PATH):
         "afd_get_info": (C.c_int, [vp, P(Info)]),
         "afd_energy": (C.c_int, [vp, i32, P(f64)]),
         "afd_set_stream": (C.c_int, [vp, vp]),
+        "afd_set_plan": (C.c_int, [vp, P(Plan)]),
         "afd_kernel_stats": (C.c_int, [vp, i32, C.c_char_p, i64, P(i64), P(f64)]),
         "afd_last_error": (C.c_char_p, [vp]),
         "afd_destroy": (None, [vp]),
@@ -439,6 +445,16 @@ class Simulation:
 
     def set_stream(self, stream_handle):
         self._check(library().afd_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def set_plan(self, tile=(0, 0), per_sm=0, dz=0, beside=False, auto=False):
+        """Fixes the streaming kernel's plan (tile in cells, resident blocks
+        per SM, z-chunk depth, boundary/PML kernels beside it) and turns the
+        online autotuner off; auto=True gives the choice back to it."""
+        if auto:
+            self._check(library().afd_set_plan(self._h, None))
+            return
+        p = Plan(tile[0], tile[1], per_sm, dz, 1 if beside else 0)
+        self._check(library().afd_set_plan(self._h, C.byref(p)))
 
     def kernel_stats(self):
         L = library()

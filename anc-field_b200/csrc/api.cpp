@@ -408,6 +408,8 @@ int afd_energy(afd_sim* s, int32_t batch, double* energy) {
 
 int afd_set_stream(afd_sim* s, void* stream) { SIM_CALL(s, s->eng->set_stream(stream)); }
 
+int afd_set_plan(afd_sim* s, const afd_plan* plan) { SIM_CALL(s, s->eng->set_plan(plan)); }
+
 int afd_kernel_stats(afd_sim* s, int32_t idx, char* name, int64_t cap, int64_t* launches, double* ms) {
     if (!s) return AFD_ERR_ARG;
     return s->eng->kernel_stats(idx, name, cap, launches, ms);

@@ -684,12 +684,13 @@ __device__ __forceinline__ void cvt8(const uint4 w, float v[8]) {
 // only its own rows. T = __half: FP16 levels, the update evaluated on the
 // stored values (slf_update_scaled) and the largest |p^n| of every work
 // item gathered for the scale of level g + 1.
-template <typename T>
+template <typename T, int S>
 __global__ void __launch_bounds__(F_THREADS, 2)
     k_stream(const __grid_constant__ CUtensorMap tm_halo, const __grid_constant__ CUtensorMap tm_own,
              const __grid_constant__ StepArgs a, const __grid_constant__ FusedDev f, int j) {
     const TlMark tl(a, 0, *a.d_step + j, true);
-    using TL = Tile<T>;
+    using TL = Tile<T, S>;
+    constexpr int F_STAGES = TL::STAGES;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + F_STAGES * TL::STAGE);
@@ -736,7 +737,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                 const int item = f.items ? __ldg(f.items + taken) : taken;
                 slot[s0] = item;
                 const FusedItem it = fused_item(f, item, nz);
-                const int x0 = it.tx * TL::W, y0 = it.ty * FT_Y;
+                const int x0 = it.tx * TL::W, y0 = it.ty * TL::H;
                 const int zc = (wc * B + it.b) * nz, zo = (wo * B + it.b) * nz;
                 for (int z = it.z0 - 1; z <= it.z1; ++z, ++k) {
                     const int s = (int)(k % F_STAGES);
@@ -762,7 +763,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
     }
 
     const int lane = tid & 31;
-    const int cx = (tid & 15) * TL::CPT, cy = tid >> 4;
+    const int cx = (tid % TL::TPR) * TL::CPT, cy = tid / TL::TPR;
     const float L2 = a.lambda2, CI = a.cint;
     uint32_t k = 0;
     while (true) {
@@ -773,7 +774,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
         const int item = slot[k % F_STAGES];
         if (item < 0) break;
         const FusedItem it = fused_item(f, item, nz);
-        const int x = it.tx * TL::W + cx, y = it.ty * FT_Y + cy;
+        const int x = it.tx * TL::W + cx, y = it.ty * TL::H + cy;
         T* pn = level_ptr<T>(a, wn) + (size_t)it.b * a.g.vol + (int64_t)y * a.g.pitch + x;
         const bool yok = (y >= 1 && y <= a.g.ny - 2);
         const bool xfull = (x >= 1 && x + TL::CPT - 1 <= a.g.nx - 2);
@@ -802,7 +803,7 @@ __global__ void __launch_bounds__(F_THREADS, 2)
                 const float4 yp = *reinterpret_cast<const float4*>(P0 + s0 + TL::HX);
                 const float4 zm = *reinterpret_cast<const float4*>(Pm + s0);
                 const float4 zp = *reinterpret_cast<const float4*>(Pp + s0);
-                const float4 o = *reinterpret_cast<const float4*>(O + cy * FT_X + cx);
+                const float4 o = *reinterpret_cast<const float4*>(O + cy * TL::W + cx);
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
                 float4 v;
@@ -953,6 +954,39 @@ __global__ void __launch_bounds__(F_THREADS, 2)
         }
         if (__any_sync(0xffffffffu, bad && yok && x <= a.g.nx - 2) && lane == 0) atomicOr(a.flag, 1);
         k += (uint32_t)planes + 2;
+    }
+}
+
+// Host view of a streaming-kernel instance: tile width and height in cells,
+// halo box width, shared memory per block and the kernel. FP16 storage has
+// no 128x8 instance: its halo box would be 272 cells wide, past the 256 a
+// TMA box allows.
+struct StreamShape {
+    int w, h, hx;
+    size_t smem;
+    const void* kern;
+};
+template <typename T, int S>
+static StreamShape stream_shape_t() {
+    using TL = Tile<T, S>;
+    static_assert(TL::HX <= 256 && TL::H + 2 <= 256, "TMA box dimensions are at most 256");
+    return StreamShape{TL::W, TL::H, TL::HX, TL::SMEM, (const void*)k_stream<T, S>};
+}
+static bool shape_valid(bool f16, int S) { return S >= 0 && S < kTileShapes && !(f16 && S == 1); }
+static StreamShape stream_shape(bool f16, int S) {
+    if (f16) return S == 2 ? stream_shape_t<__half, 2>() : stream_shape_t<__half, 0>();
+    return S == 1 ? stream_shape_t<float, 1>() : (S == 2 ? stream_shape_t<float, 2>() : stream_shape_t<float, 0>());
+}
+template <typename T>
+static void launch_stream(int S, int grid, cudaStream_t st, const CUtensorMap& th, const CUtensorMap& to,
+                          const StepArgs& a, const FusedDev& f, int j) {
+    if constexpr (sizeof(T) == 2) {
+        if (S == 2) k_stream<T, 2><<<grid, F_THREADS, Tile<T, 2>::SMEM, st>>>(th, to, a, f, j);
+        else k_stream<T, 0><<<grid, F_THREADS, Tile<T, 0>::SMEM, st>>>(th, to, a, f, j);
+    } else {
+        if (S == 1) k_stream<T, 1><<<grid, F_THREADS, Tile<T, 1>::SMEM, st>>>(th, to, a, f, j);
+        else if (S == 2) k_stream<T, 2><<<grid, F_THREADS, Tile<T, 2>::SMEM, st>>>(th, to, a, f, j);
+        else k_stream<T, 0><<<grid, F_THREADS, Tile<T, 0>::SMEM, st>>>(th, to, a, f, j);
     }
 }
 
@@ -1243,7 +1277,7 @@ struct Engine::Impl {
     DBuf<int> f_work;
     // compact work lists of the streaming kernel (FIXED scheme), one per plan
     struct PlanItems {
-        std::array<int64_t, 6> key{{-1, -1, -1, -1, -1, -1}};
+        std::array<int64_t, 7> key{{-1, -1, -1, -1, -1, -1, -1}};
         int64_t n = -1;  // -1: every item
         DBuf<int> buf;
     };
@@ -1254,13 +1288,15 @@ struct Engine::Impl {
     // kernel then skips so that those kernels can run beside it
     DBuf<uint32_t> lrs_bits, pml_owned, owned;
     bool owned_dirty = true;
-    // streaming plan: resident blocks per SM (0: as many as fit) and z-chunk
+    // streaming plan: tile shape (0: 64x16, 1: 128x8, 2: 32x32 cells for
+    // FP32 storage), resident blocks per SM (0: as many as fit) and z-chunk
     // depth (0: the rule in build_fused); the online autotuner picks them
     struct Plan {
         int per_sm, dz;
         bool beside;  // boundary and PML pressure kernels beside the streaming kernel
+        int shape;
     };
-    Plan plan{0, 0, false};
+    Plan plan{0, 0, false, 0};
     std::vector<Plan> tune_cands;
     std::vector<float> tune_ms;
     size_t tune_next = 0;
@@ -1270,41 +1306,59 @@ struct Engine::Impl {
     cudaEvent_t tev0 = nullptr, tev1 = nullptr;
     bool tune_active() const { return use_fused() && prm.graphs && !prm.profile && !tuned; }
     void apply_plan(int id) {
-        plan = id == 0 ? Plan{0, 0, false} : tune_cands[(size_t)id - 1];
+        plan = id == 0 ? Plan{0, 0, false, 0} : tune_cands[(size_t)id - 1];
         plan_id = id;
         fused_dirty = true;
         build_fused();
     }
-    // candidates: the streaming kernel alone with all resident blocks per SM
-    // and z-chunk depth {rule, rule / 2, rule / 4}, or (FP32 storage) beside the
-    // boundary and PML kernels with {all, all - 1} blocks per SM; every
-    // candidate gives the results of the serial order
-    // candidates of the current model and grid, made once (the plan then
-    // restarts from the default)
+    // candidates: for each tile shape the streaming kernel alone with all
+    // resident blocks per SM and z-chunk depth {rule, rule / 4} (and rule / 2
+    // for the 64x16 tile), or (FP32 storage, 64x16 tile) beside the boundary
+    // and PML kernels with {all, all - 1} blocks per SM; every candidate gives
+    // the results of the serial order. Made once per model and grid (the plan
+    // then restarts from the default).
     void ensure_candidates() {
         if (use_fused() && tune_gen != model_gen) {
             make_candidates();
-            apply_plan(0);
+            apply_plan(forced ? 1 : 0);
         }
     }
+    // a plan fixed by afd_set_plan: the only candidate, tuning off
+    bool forced = false;
+    Plan forced_plan{0, 0, false, 0};
+    // resident blocks per SM that fit and the z-chunk depth rule of a shape
+    void shape_limits(int shape, int* per_sm_max, int* dz_rule);
     void make_candidates() {
         tune_cands.clear();
-        auto add = [&](int ps, int d, bool bs) {
+        if (forced) {
+            tune_cands.push_back(forced_plan);
+            tune_ms.assign(1, 0.0f);
+            tune_next = 1;
+            tuned = true;
+            tune_gen = model_gen;
+            return;
+        }
+        auto add = [&](int ps, int d, bool bs, int sh) {
             if (ps < 1 || d < 8) return;
             for (const Plan& q : tune_cands)
-                if (q.per_sm == ps && q.dz == d && q.beside == bs) return;
-            tune_cands.push_back(Plan{ps, d, bs});
+                if (q.per_sm == ps && q.dz == d && q.beside == bs && q.shape == sh) return;
+            tune_cands.push_back(Plan{ps, d, bs, sh});
         };
-        add(max_per_sm, rule_dz, false);
-        add(max_per_sm, rule_dz / 2, false);
-        add(max_per_sm, rule_dz / 4, false);
-        // the plans with the boundary and PML kernels beside the streaming
-        // kernel are offered for FP32 storage only: with FP16 storage they
-        // gave results that differed from the serial order and between runs
-        // (16-member batch), so FP16 runs keep the serial order
-        if (owned.ptr && !ref() && !f16()) {
-            add(max_per_sm, rule_dz, true);
-            add(max_per_sm - 1, rule_dz, true);
+        for (int sh = 0; sh < kTileShapes; ++sh) {
+            if (!shape_valid(f16(), sh)) continue;
+            int ps = 0, rule = 0;
+            shape_limits(sh, &ps, &rule);
+            add(ps, rule, false, sh);
+            if (sh == 0) add(ps, rule / 2, false, sh);
+            add(ps, rule / 4, false, sh);
+            // the plans with the boundary and PML kernels beside the streaming
+            // kernel are offered for FP32 storage only: with FP16 storage they
+            // gave results that differed from the serial order and between
+            // runs (16-member batch), so FP16 runs keep the serial order
+            if (sh == 0 && owned.ptr && !ref() && !f16()) {
+                add(ps, rule, true, sh);
+                add(ps - 1, rule, true, sh);
+            }
         }
         tune_ms.assign(tune_cands.size(), 0.0f);
         tune_next = 0;
@@ -1323,13 +1377,13 @@ struct Engine::Impl {
         }
         return sb;
     }
-    std::array<int64_t, 4> flags_key{{-1, -1, -1, -1}};
+    std::array<int64_t, 5> flags_key{{-1, -1, -1, -1, -1}};
     int64_t model_gen = 0;  // counts init_device calls (a new model or grid)
     CUtensorMap tm_halo{}, tm_own{};
     int fused_grid = 0;
-    int max_per_sm = 0, rule_dz = 0;
+    int max_per_sm = 0, rule_dz = 0, stream_per_sm = 0;
     bool fused_dirty = true;
-    int tiles_x = 0, tiles_y = 0;
+    int tiles_x = 0, tiles_y = 0, tile_w = 0, tile_h = 0;
 
     StepArgs args{};
     SrcRcvInline inl{};
@@ -1391,6 +1445,8 @@ struct Engine::Impl {
         return pinned;
     }
     void build_fused();
+    void encode_maps(int shape);
+    int maps_shape = -1;  // shape of tm_halo / tm_own (-1: none yet for these buffers)
     bool use_fused() const { return prm.fused != 0; }
     // FIXED scheme in graphs: the boundary and PML pressure kernels run
     // beside the streaming kernel (which skips the cells they own)
@@ -1467,9 +1523,6 @@ void Engine::Impl::init_device() {
         if (!f16_smax.ptr) f16_smax.alloc((size_t)prm.batch);
     }
 
-    const int tile_w = f16() ? Tile<__half>::W : Tile<float>::W;
-    tiles_x = (nx + tile_w - 1) / tile_w;
-    tiles_y = (ny + FT_Y - 1) / FT_Y;
     // boundary list, sorted by (tile, plane, position in tile) so that the
     // boundary kernel's neighbour reads stay local; every order gives the
     // same results. The list arrives in z-y-x scan order, in which the cells
@@ -1508,32 +1561,7 @@ void Engine::Impl::init_device() {
         coef_a.upload(model.a);
         coef_b.upload(model.b);
     }
-    // tensor maps over the three field levels seen as one stack of
-    // 3 * batch * nz planes: the halo box of p^n and the own box of p^{n-1}
-    {
-        typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
-                                     CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                                     CUtensorMapFloatOOBfill);
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-        if (!fn || q != cudaDriverEntryPointSuccess) throw Error(AFD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        EncodeFn enc = (EncodeFn)fn;
-        const cuuint64_t es = f16() ? 2 : 4;
-        const CUtensorMapDataType dt = f16() ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-        const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)(3 * prm.batch * nz)};
-        const cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)plane * es};
-        const cuuint32_t box_h[3] = {(cuuint32_t)(f16() ? Tile<__half>::HX : Tile<float>::HX), FH_Y, 1},
-                         box_o[3] = {(cuuint32_t)tile_w, FT_Y, 1}, estr[3] = {1, 1, 1};
-        CUresult r1 = enc(&tm_halo, dt, 3, fields.ptr, dims, strides, box_h, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        CUresult r2 = enc(&tm_own, dt, 3, fields.ptr, dims, strides, box_o, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) throw Error(AFD_ERR_CUDA, "tensor map encoding failed");
-    }
+    maps_shape = -1;  // the tensor maps cover the new field buffers once build_fused encodes them
     initialized = true;
     fused_dirty = true;
     owned_dirty = true;
@@ -1553,32 +1581,80 @@ void Engine::Impl::build_owned_mask() {
     CK(cudaStreamSynchronize(stream));
 }
 
+// Tensor maps over the three field levels seen as one stack of
+// 3 * batch * nz planes: the halo box of p^n and the own box of p^{n-1} of
+// a tile of the given shape.
+void Engine::Impl::encode_maps(int shape) {
+    typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) throw Error(AFD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    EncodeFn enc = (EncodeFn)fn;
+    const StreamShape sh = stream_shape(f16(), shape);
+    const cuuint64_t es = f16() ? 2 : 4;
+    const CUtensorMapDataType dt = f16() ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)(3 * prm.batch * nz)};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)plane * es};
+    const cuuint32_t box_h[3] = {(cuuint32_t)sh.hx, (cuuint32_t)(sh.h + 2), 1},
+                     box_o[3] = {(cuuint32_t)sh.w, (cuuint32_t)sh.h, 1}, estr[3] = {1, 1, 1};
+    CUresult r1 = enc(&tm_halo, dt, 3, fields.ptr, dims, strides, box_h, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r2 = enc(&tm_own, dt, 3, fields.ptr, dims, strides, box_o, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) throw Error(AFD_ERR_CUDA, "tensor map encoding failed");
+    maps_shape = shape;
+}
+
+// z-chunk depth: enough work items for every resident block to take a few,
+// with the two halo planes a small share of each chunk.
+static int chunk_rule(int64_t tiles, int nz, int64_t resident) {
+    int dz = 64;
+    while (dz > 8 && tiles * ((nz - 2 + dz - 1) / dz) < 4 * resident) dz /= 2;
+    return dz;
+}
+
+void Engine::Impl::shape_limits(int shape, int* per_sm_max, int* dz_rule) {
+    const StreamShape sh = stream_shape(f16(), shape);
+    int per_sm = 0, sms = 0;
+    CK(cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sh.kern, F_THREADS, sh.smem));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    per_sm = std::max(per_sm, 1);
+    const int64_t tiles = (int64_t)((nx + sh.w - 1) / sh.w) * ((ny + sh.h - 1) / sh.h) * prm.batch;
+    *per_sm_max = per_sm;
+    *dz_rule = chunk_rule(tiles, nz, (int64_t)per_sm * sms);
+}
+
 // Work decomposition of the streaming kernel: tiles, z-chunk depth and the
 // persistent grid size.
 void Engine::Impl::build_fused() {
     FusedDev& F = fdev;
     F = FusedDev{};
+    if (!shape_valid(f16(), plan.shape)) plan.shape = 0;
+    const StreamShape sh = stream_shape(f16(), plan.shape);
+    tile_w = sh.w;
+    tile_h = sh.h;
+    tiles_x = (nx + sh.w - 1) / sh.w;
+    tiles_y = (ny + sh.h - 1) / sh.h;
+    if (maps_shape != plan.shape) encode_maps(plan.shape);
     F.tiles_x = tiles_x;
     F.tiles_y = tiles_y;
     int per_sm = 0;
-    const void* kern = f16() ? (const void*)k_stream<__half> : (const void*)k_stream<float>;
-    const size_t smem = f16() ? Tile<__half>::SMEM : Tile<float>::SMEM;
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, F_THREADS, smem));
+    CK(cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sh.kern, F_THREADS, sh.smem));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    // with the boundary and PML kernels beside it, one block slot per SM is
-    // left free for them
     max_per_sm = std::max(per_sm, 1);
     if (plan.per_sm > 0) per_sm = std::min(per_sm, plan.per_sm);
-    const int64_t resident = (int64_t)std::max(per_sm, 1) * sms;
+    stream_per_sm = std::max(per_sm, 1);
+    const int64_t resident = (int64_t)stream_per_sm * sms;
     F.owned = lists_beside() ? owned.ptr : nullptr;
     F.owned_wpr = (int32_t)(pitch / 32);
     const int64_t tiles = (int64_t)tiles_x * tiles_y * prm.batch;
-    // z-chunk depth: enough work items for every resident block to take a
-    // few, with the two halo planes a small share of each chunk
-    int dz = 64;
-    while (dz > 8 && tiles * ((nz - 2 + dz - 1) / dz) < 4 * resident) dz /= 2;
+    int dz = chunk_rule(tiles, nz, resident);
     rule_dz = dz;
     if (plan.dz > 0) dz = plan.dz;
     F.dz = dz;
@@ -1594,20 +1670,20 @@ void Engine::Impl::build_fused() {
     // the work list depends on the model, the tiling, the batch and the
     // plan's z-chunk depth; one device copy per plan lives as long as the
     // engine, because the graphs of every tried plan keep its address
-    const std::array<int64_t, 6> key = {model_gen, tiles_x, tiles_y, dz, prm.batch, f16() ? 1 : 0};
+    const std::array<int64_t, 7> key = {model_gen, tiles_x, tiles_y, dz, prm.batch, f16() ? 1 : 0, plan.shape};
     PlanItems& pi = plan_items[plan_id];
     if (pi.key != key && !ref() && have_model) {
         pi.key = key;
         pi.n = -1;
-        const int W = f16() ? Tile<__half>::W : Tile<float>::W;
+        const int W = sh.w;
         const int64_t ntile = (int64_t)tiles_x * tiles_y;
-        const std::array<int64_t, 4> fkey = {model_gen, tiles_x, tiles_y, W};
+        const std::array<int64_t, 5> fkey = {model_gen, tiles_x, tiles_y, W, sh.h};
         if (fkey != flags_key) {
             flags_key = fkey;
             air_flags.assign((size_t)(ntile * nz), 0);
             DBuf<uint8_t> fl;
             fl.alloc(air_flags.size(), false);
-            air_flags_device(solid_view(), nx, ny, nz, W, FT_Y, tiles_x, tiles_y, fl.ptr, stream);
+            air_flags_device(solid_view(), nx, ny, nz, W, sh.h, tiles_x, tiles_y, fl.ptr, stream);
             CK(cudaMemcpyAsync(air_flags.data(), fl.ptr, air_flags.size(), cudaMemcpyDeviceToHost, stream));
             CK(cudaStreamSynchronize(stream));
         }
@@ -1954,7 +2030,7 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
     };
     const dim3 blk(64, 4, 1);
     auto stream_launch = [&](cudaStream_t st) {
-        k_stream<T><<<fused_grid, F_THREADS, Tile<T>::SMEM, st>>>(tm_halo, tm_own, a, fdev, j);
+        launch_stream<T>(plan.shape, fused_grid, st, tm_halo, tm_own, a, fdev, j);
         ++launches;
     };
     const bool beside = lists_beside() && fdev.owned;
@@ -2224,6 +2300,35 @@ void Engine::set_stream(void* stream) {
         D.drop_graphs();
         D.stream = s;
     }
+}
+
+void Engine::set_plan(const afd_plan* p) {
+    Impl& D = *d_;
+    int shape = 0;
+    if (p) {
+        shape = -1;
+        if (p->tile_x == 0 && p->tile_y == 0) shape = 0;
+        for (int sh = 0; sh < kTileShapes && shape < 0; ++sh)
+            if (shape_valid(D.f16(), sh) && p->tile_x == shape_w32(sh) * (D.f16() ? 2 : 1) && p->tile_y == shape_h(sh))
+                shape = sh;
+        if (shape < 0)
+            throw Error(AFD_ERR_ARG, D.f16() ? "unsupported streaming tile (FP16 storage: 128x16 or 64x32)"
+                                             : "unsupported streaming tile (64x16, 128x8 or 32x32)");
+        if (p->per_sm < 0 || p->per_sm > 32) throw Error(AFD_ERR_ARG, "per_sm out of range (0..32)");
+        if (p->dz < 0 || p->dz > 1024) throw Error(AFD_ERR_ARG, "dz out of range (0..1024)");
+    }
+    CK(cudaSetDevice(D.device));
+    CK(cudaStreamSynchronize(D.stream));
+    // no graph may keep the addresses of the per-plan work lists freed here
+    D.drop_graphs();
+    D.plan_items.clear();
+    D.forced = p != nullptr;
+    if (p) D.forced_plan = Impl::Plan{p->per_sm, p->dz, p->beside != 0, shape};
+    D.tuned = false;
+    D.tune_gen = -1;  // candidates are made again by the next run or prepare
+    D.plan = Impl::Plan{0, 0, false, 0};
+    D.plan_id = 0;
+    D.fused_dirty = true;
 }
 
 void Engine::set_min_size(float x, float y, float z) {
@@ -2800,11 +2905,12 @@ void Engine::get_info(afd_info* info) {
     info->storage = D.prm.storage;
     info->last_run_ms = D.last_ms;
     info->kernel_launches = D.launches;
-    info->tile_x = D.f16() ? Tile<__half>::W : Tile<float>::W;
-    info->tile_y = FT_Y;
+    info->tile_x = D.tile_w;
+    info->tile_y = D.tile_h;
     info->tile_z = D.fdev.dz;
     info->stream_blocks = D.fused_grid;
     info->stream_beside = D.lists_beside() ? 1 : 0;
+    info->stream_per_sm = D.stream_per_sm;
     info->tuned = D.tuned ? 1 : 0;
 }
 

@@ -47,6 +47,7 @@ public:
     void get_info(afd_info* info);
     double energy(int32_t batch);
     void set_stream(void* stream);
+    void set_plan(const afd_plan* plan);
     float cell_size() const;
     int kernel_stats(int32_t idx, char* name, int64_t cap, int64_t* launches, double* ms);
 

@@ -4,7 +4,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -115,12 +114,22 @@ void check_filters(int32_t nmat, int32_t K, const double* a, const double* b, in
     const bool gpu = cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0;
     if (gpu) {
         const int blocks = 8;
-        double *da, *db, *dr, *dl;
+        // freed on every path, a failed allocation included
+        struct Bufs {
+            double *a = nullptr, *b = nullptr, *r = nullptr, *l = nullptr;
+            ~Bufs() {
+                cudaFree(a);
+                cudaFree(b);
+                cudaFree(r);
+                cudaFree(l);
+            }
+        } m;
         const size_t nab = (size_t)nmat * K;
-        CKF(cudaMalloc(&da, nab * sizeof(double)));
-        CKF(cudaMalloc(&db, nab * sizeof(double)));
-        CKF(cudaMalloc(&dr, (size_t)nmat * sizeof(double)));
-        CKF(cudaMalloc(&dl, (size_t)nmat * blocks * sizeof(double)));
+        CKF(cudaMalloc(&m.a, nab * sizeof(double)));
+        CKF(cudaMalloc(&m.b, nab * sizeof(double)));
+        CKF(cudaMalloc(&m.r, (size_t)nmat * sizeof(double)));
+        CKF(cudaMalloc(&m.l, (size_t)nmat * blocks * sizeof(double)));
+        double *da = m.a, *db = m.b, *dr = m.r, *dl = m.l;
         CKF(cudaMemcpy(da, a, nab * sizeof(double), cudaMemcpyHostToDevice));
         CKF(cudaMemcpy(db, b, nab * sizeof(double), cudaMemcpyHostToDevice));
         k_roots<<<(nmat + 63) / 64, 64>>>(db, nmat, K, dr);
@@ -129,13 +138,11 @@ void check_filters(int32_t nmat, int32_t K, const double* a, const double* b, in
         std::vector<double> part((size_t)nmat * blocks);
         CKF(cudaMemcpy(roots.data(), dr, (size_t)nmat * sizeof(double), cudaMemcpyDeviceToHost));
         CKF(cudaMemcpy(part.data(), dl, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        for (int m = 0; m < nmat; ++m)
-            for (int k = 0; k < blocks; ++k) lows[(size_t)m] = std::fmin(lows[(size_t)m], part[(size_t)m * blocks + k]);
-        cudaFree(da);
-        cudaFree(db);
-        cudaFree(dr);
-        cudaFree(dl);
+        for (int i = 0; i < nmat; ++i)
+            for (int k = 0; k < blocks; ++k) lows[(size_t)i] = std::fmin(lows[(size_t)i], part[(size_t)i * blocks + k]);
     } else {
+        // no CUDA device: the same FP64 arithmetic on the host (a coefficient
+        // check before a run, not part of the step)
         for (int m = 0; m < nmat; ++m) {
             roots[(size_t)m] = max_root_of(b + (size_t)m * K, K);
             for (int f = 0; f < nf; ++f) {
@@ -158,16 +165,21 @@ void check_filters(int32_t nmat, int32_t K, const double* a, const double* b, in
 // Allocation-free variant of the filter check.
 //
 // For callers that must not allocate device memory: a process that runs
-// under a fixed GPU memory budget set by its host application, or a
-// control thread that re-checks filter coefficients while a simulation is
-// running and may not grow or fragment the device heap. The scratch lives
-// in one file-scope device array; inputs and outputs stay host arrays.
+// under a fixed GPU memory budget set by its host application (which has
+// reserved the device memory for itself), or a setup path that re-checks
+// filter coefficients after the simulations have taken the rest of the
+// device and a cudaMalloc could fail. The scratch lives in one file-scope
+// device array; inputs and outputs stay host arrays.
 // Limits: nmat <= kStaticMaxMat materials, ncoef <= kStaticMaxCoef.
 // Every call reuses the same array, so calls that overlap on the GPU (from
-// several host threads, or on a device in use by another such call) race
-// and must be serialised by the caller. The first call on a device looks up
-// the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture.
+// several host threads on one device) race and must be serialised by the
+// caller. The copies are synchronous cudaMemcpy calls and the kernels go to
+// the legacy default stream, so a call waits for work queued on that
+// device's blocking streams (the simulation engine's own streams are
+// non-blocking). Each call looks up the array's device address
+// (cudaGetSymbolAddress) with the device current: an address kept from an
+// earlier call would be stale after a cudaDeviceReset. The first call on a
+// device loads the module there; make it before any stream capture.
 // ---------------------------------------------------------------------------
 constexpr int kStaticMaxMat = 64;
 constexpr int kStaticMaxCoef = 16;
@@ -176,23 +188,13 @@ constexpr int kStaticDoubles =
     2 * kStaticMaxMat * kStaticMaxCoef + kStaticMaxMat + kStaticMaxMat * kStaticBlocks;
 static __device__ __align__(256) double g_filter_scratch[kStaticDoubles];
 
-static std::mutex g_scratch_mu;
-static double* g_scratch_ptr[256] = {};
-
-// Device address of g_filter_scratch on the current device (set up once).
+// Device address of g_filter_scratch on the current device.
 static double* scratch_on_current_device() {
-    int dev = 0;
-    CKF(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 256) throw Error(AFD_ERR_CUDA, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_filter_scratch);
-        if (e != cudaSuccess || !ptr)
-            throw Error(AFD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<double*>(ptr);
-    }
-    return g_scratch_ptr[dev];
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_filter_scratch);
+    if (e != cudaSuccess || !ptr)
+        throw Error(AFD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return static_cast<double*>(ptr);
 }
 
 void check_filters_static(int32_t nmat, int32_t K, const double* a, const double* b, int32_t nf,

@@ -20,45 +20,45 @@
 
 namespace afd {
 
-constexpr int FT_X = 64;                 // tile width in x (cells)
-constexpr int FT_Y = 16;                 // tile height in y
-constexpr int FH_X = FT_X + 8;           // halo tile width (4-cell aligned halo each side)
-constexpr int FH_Y = FT_Y + 2;
-constexpr int F_STAGES = 8;
-constexpr int F_PN_BYTES = FH_X * FH_Y * 4;                 // 5184
-constexpr int F_PN_PAD = (F_PN_BYTES + 127) / 128 * 128;    // 5248
-constexpr int F_PO_BYTES = FT_X * FT_Y * 4;                 // 4096
-constexpr int F_STAGE_BYTES = F_PN_PAD + F_PO_BYTES;        // 9344
-constexpr int F_TX_BYTES = F_PN_BYTES + F_PO_BYTES;         // bytes each stage receives
+constexpr int FT_X = 64;                 // default tile width in x (cells, FP32 storage)
+constexpr int FT_Y = 16;                 // default tile height in y
 constexpr int F_CONSUMERS = 256;
 constexpr int F_THREADS = F_CONSUMERS + 32;
-constexpr size_t F_SMEM = (size_t)F_STAGES * F_STAGE_BYTES + 2 * F_STAGES * 8 + F_STAGES * 4 + 128;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s
 
-// Stage layout per storage type. FP16 levels: 128-cell tiles (a stage
-// holds the same bytes as an FP32 one), the halo box starts 8 cells before
-// the tile (x times 2 bytes stays a multiple of 16) and is 144 cells wide.
-template <typename T>
-struct Tile;
-// W: tile width in cells; CPT: cells per consumer thread (16 threads per
-// row, 16 rows).
-template <>
-struct Tile<float> {
-    static constexpr int W = FT_X, CPT = 4;
-    static constexpr int HX = FH_X, XOFF = 4, PN_PAD = F_PN_PAD, STAGE = F_STAGE_BYTES, TX = F_TX_BYTES;
-    static constexpr size_t SMEM = F_SMEM;
+// Tile shapes of the streaming kernel (a plan parameter the autotuner
+// varies): S = 0: 64 x 16, 1: 128 x 8, 2: 32 x 32 cells for FP32 storage;
+// FP16 storage doubles the width (the same bytes per row).
+constexpr int kTileShapes = 3;
+__host__ __device__ constexpr int shape_w32(int S) { return S == 0 ? 64 : (S == 1 ? 128 : 32); }
+__host__ __device__ constexpr int shape_h(int S) { return S == 0 ? 16 : (S == 1 ? 8 : 32); }
+
+// Stage layout per storage type and shape. W: tile width in cells; H: rows;
+// CPT: cells per consumer thread; TPR = W / CPT consumer threads per row
+// (TPR x H = 256). The p^n box is the tile with a one-cell halo in y and a
+// halo of XOFF cells in x (x times the element size stays a multiple of 16
+// bytes, as TMA requires), followed by the p^{n-1} box of the tile. The
+// 64 x 16 shape keeps 8 stages; the others, whose halo boxes are larger,
+// keep 7 so that three blocks still fit an SM's shared memory.
+template <typename T, int S = 0>
+struct Tile {
+    static constexpr int ES = (int)sizeof(T);
+    static constexpr int CPT = ES == 4 ? 4 : 8;
+    static constexpr int W = shape_w32(S) * (4 / ES);
+    static constexpr int H = shape_h(S);
+    static constexpr int TPR = W / CPT;
+    static constexpr int XOFF = 16 / ES;
+    static constexpr int HX = W + 2 * XOFF;
+    static constexpr int PN_BYTES = HX * (H + 2) * ES;
+    static constexpr int PN_PAD = (PN_BYTES + 127) / 128 * 128;
+    static constexpr int PO_BYTES = W * H * ES;
+    static constexpr int STAGE = (PN_PAD + PO_BYTES + 127) / 128 * 128;
+    static constexpr int TX = PN_BYTES + PO_BYTES;  // bytes each stage receives
+    static constexpr int STAGES = S == 0 ? 8 : 7;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 2 * STAGES * 8 + STAGES * 4 + 128;
+    static_assert(TPR * H == F_CONSUMERS, "256 consumer threads cover the tile");
 };
-template <>
-struct Tile<__half> {
-    static constexpr int W = 2 * FT_X, CPT = 8;
-    static constexpr int HX = W + 16, XOFF = 8;
-    static constexpr int PN_BYTES = HX * FH_Y * 2;                               // 5184
-    static constexpr int PN_PAD = (PN_BYTES + 127) / 128 * 128;                  // 5248
-    static constexpr int PO_BYTES = W * FT_Y * 2;                                // 4096
-    static constexpr int STAGE = (PN_PAD + PO_BYTES + 127) / 128 * 128;          // 9344
-    static constexpr int TX = PN_BYTES + PO_BYTES;                               // 9280
-    static constexpr size_t SMEM = (size_t)F_STAGES * STAGE + 2 * F_STAGES * 8 + F_STAGES * 4 + 128;
-};
+static_assert(Tile<float, 0>::STAGE == 9344 && Tile<float, 0>::TX == 9280, "64 x 16 FP32 stage");
 
 // Work decomposition of the streaming kernel.
 struct FusedDev {

@@ -41,8 +41,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None,
                     help="NX,NY,NZ: the same construction at another size (profiling captures)")
-    ap.add_argument("--legs", default="device,e2e,timeline,roofline,cpu",
-                    help="comma list of device,e2e,roofline,cpu")
+    ap.add_argument("--legs", default="device,e2e,timeline,roofline,parity,cpu",
+                    help="comma list of device,e2e,timeline,roofline,parity,cpu")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c3rooms", "c5", "lms", "gemm"],
                     help="c2: the single-source throughput line (default); c3: batched secondary-path IRs/s; "
                          "c3rooms: 8 uneven rooms in one launch; "
@@ -66,18 +66,63 @@ def peaks():
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock and the clock-event (throttle) reasons of one GPU
+    during the timed region: through NVML every ~2 ms (a timed region of a
+    few milliseconds still gets samples), else nvidia-smi every 200 ms."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8 | 0x80, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []
+        self.stop_flag = False
+        self.max_mhz = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        h = None
+        try:
+            # the CUDA device's UUID: NVML numbers the GPUs of the machine,
+            # which differs from CUDA's ordinal under CUDA_VISIBLE_DEVICES
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+        except Exception:
+            h = None
+        if h is None:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        return pynvml, h
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.nvml = (nv, h)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self.stop_flag:
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             int(reasons(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+            self.th = threading.Thread(target=poll, daemon=True)
+            self.th.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -92,6 +137,13 @@ class Clocks:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml:
+            self.stop_flag = True
+            self.th.join(timeout=2)
+            sm = [v for v, _ in self.samples]
+            reasons = sorted(k for k, bit in self.BITS.items() if any(r & bit for _, r in self.samples))
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -114,7 +166,7 @@ class Clocks:
                 if f[5 + k].lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def max_over_ranks(value, device="cpu"):
@@ -142,38 +194,53 @@ def dist_env():
     return rank, world, local
 
 
-def cpu_reference(cfg, steps, budget_s=25.0, precision="f32"):
-    """Times the reference's own kernels (oracle/_ref, REF semantics, no PML
-    kernel) on the workload's geometry with all host threads. The sample is
-    a z-slab of the grid sized to about budget_s seconds in total."""
+def cpu_reference(cfg, steps=50, repeats=3, zs=64):
+    """Times the reference's own kernels (oracle/_ref: leapfrog.cl, the 26
+    lrs_*.cl launches, pml.cl when the workload has a PML, source.cl, mic.cl)
+    with every host thread, on a zs-plane z-slab of the workload grid closed
+    by a wall on top. The reference has one PML form, the whole-interior
+    kernel of pml.cl:154-265 (its face profile only sets ksi), so a workload
+    with PML slabs runs that kernel over every cell, its NDRange spread over
+    the threads as a CPU OpenCL device runs it. Per-step time from the
+    harness's step-loop timer (set-up excluded), median of `repeats` runs of
+    `steps` steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    impl = "ref" if oracle.available("ref", precision) else "ora"
+    import ancfield_b200.workloads as W
     nx, ny, nz = cfg.dims
-    # one probe step on a thin slab to size the sample
-    def run_slab(zs, n):
-        vox = cfg.vox[:zs].copy()
-        vox[-1] = np.where(vox[-1] == -1, 0, vox[-1])  # close the slab with a wall
-        import ancfield_b200.workloads as W
-        vox = W.close_gaps(vox)
-        src = [((cfg.sources[0][0][0], cfg.sources[0][0][1], min(cfg.sources[0][0][2], zs - 3)),
-                cfg.sources[0][1][:n])]
-        rcv = [(r[0], r[1], min(r[2], zs - 2)) for r in cfg.receivers]
-        t = time.perf_counter()
-        oracle.simulate((nx, ny, zs), vox, cfg.a, cfg.b, dx=cfg.dx, c=cfg.c, dt=cfg.dt, mode=0,
-                        sources=src, receivers=rcv, steps=n, impl=impl)
-        return time.perf_counter() - t
-    zs = min(nz, 16)
-    t1 = run_slab(zs, 2)
-    per_cell_step = t1 / (2 * nx * ny * zs)
-    zs = int(max(8, min(nz, budget_s / max(steps, 1) / (per_cell_step * nx * ny))))
-    t = run_slab(zs, steps)
+    zs = min(zs, nz)
+    vox = cfg.vox[:zs].copy()
+    vox[-1] = np.where(vox[-1] == -1, 0, vox[-1])  # close the slab with a wall
+    vox = W.close_gaps(vox)
+    src = [((cfg.sources[0][0][0], cfg.sources[0][0][1], min(cfg.sources[0][0][2], zs - 3)),
+            np.resize(cfg.sources[0][1], steps))]
+    rcv = [(r[0], r[1], min(r[2], zs - 2)) for r in cfg.receivers]
+    pml = cfg.pml_width if cfg.pml_width else 0
+    ksi = W.ksi_arrays((nx, ny, zs), pml, cfg.pml_faces) if pml else None
     cells = (nx - 2) * (ny - 2) * (zs - 2)
+    if oracle.available("ref", "f32"):
+        impl, kind = "ref", "reference"
+        loop_s = oracle.ref_timing(True)
+    else:
+        impl, kind, loop_s = "ora", "port", None
+    times = []
+    try:
+        for _ in range(repeats):
+            t = time.perf_counter()
+            oracle.simulate((nx, ny, zs), vox, cfg.a, cfg.b, dx=cfg.dx, c=cfg.c, dt=cfg.dt, mode=0,
+                            pml_width=pml, faces=63, ksi=ksi, sources=src, receivers=rcv, steps=steps, impl=impl)
+            times.append(loop_s() if loop_s else time.perf_counter() - t)
+    finally:
+        if loop_s:
+            oracle.ref_timing(False)  # parity users of the harness get the serial PML order back
+    t = statistics.median(times)
     return {"value": cells * steps / t / 1e6, "unit": "Mcell-updates/s", "cores": os.cpu_count(),
-            "kind": "reference" if impl == "ref" else "port",
-            "sample": "%dx%dx%d slab of the workload grid, %d steps, reference kernels leapfrog+26 LRS+"
-                      "source+mic (REF semantics, PML kernel not run), OpenMP %d threads, %.1f s"
-                      % (nx, ny, zs, steps, os.cpu_count(), t)}
+            "kind": kind,
+            "sample": "%dx%dx%d z-slab of the workload grid, %d steps, median of %d runs (%s s), step loop only; "
+                      "the reference's kernels leapfrog + 26 LRS%s + source + mic in REF semantics, OpenMP %d "
+                      "threads" % (nx, ny, zs, steps, repeats, ", ".join("%.2f" % v for v in times),
+                                   " + its whole-interior PML kernel (width %d; the GPU arm updates the PML "
+                                   "slabs only, FIXED scheme)" % pml if pml else "", os.cpu_count())}
 
 
 def bench_c3(pkg, args):
@@ -470,7 +537,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        cb = cpu_reference(cfg, max(args.steps, 1) + max(args.warmup, 0), budget_s=90.0)
+        cb = cpu_reference(cfg)
         line = {"metric": metric, "value": cb["value"], "unit": cb["unit"], "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "impl": "reference", "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -531,9 +598,11 @@ def main():
     line = {"metric": metric, "value": value, "unit": metric, "n_gpus": world, "steps": K, "warmup": Wm,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "plan": {"tile": [sim.info().tile_x, sim.info().tile_y, sim.info().tile_z],
-                     "stream_blocks": sim.info().stream_blocks, "beside": bool(sim.info().stream_beside),
-                     "tuned": bool(sim.info().tuned)},
+                     "stream_blocks": sim.info().stream_blocks, "per_sm": sim.info().stream_per_sm,
+                     "beside": bool(sim.info().stream_beside), "tuned": bool(sim.info().tuned)},
             "dtype": "f32", "data": "synthetic", "config": config, "gpu_launches": launches, "clocks": clk}
+    info = sim.info()
+    step_bytes, step_parts = step_algorithmic_bytes(info, 6.0 if f16 else 12.0, interior)
     if "e2e" in legs:
         line["e2e"] = e2e_leg(sim, cfg, K, interior, world, metric)
     if "timeline" in legs:
@@ -542,8 +611,14 @@ def main():
     if "roofline" in legs:
         line["roofline"] = roofline_leg(make_sim, K, interior, 6.0 if f16 else 12.0,
                                         traffic_key=(tuple(cfg.dims), "fp16" if f16 else "fp32"))
+        peak = line["roofline"]["peak"]
+        line["roofline"]["step"] = {"bytes": step_bytes, "parts": step_parts,
+                                    "achieved": step_bytes / (ms / K / 1e3) / 1e9, "unit": "GB/s",
+                                    "frac": step_bytes / (ms / K / 1e3) / 1e9 / peak}
+    if "parity" in legs and rank == 0:
+        line["parity"] = parity_leg(make_sim, cfg, info, f16)
     if rank == 0 and world == 1 and "cpu" in legs and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(cfg, 4)
+        line["cpu_baseline"] = cpu_reference(cfg)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -551,6 +626,52 @@ def main():
 
 
 TIMELINE_RUN = 240  # steps of the timeline leg (32 recorded)
+
+
+def step_algorithmic_bytes(info, interior_bytes, interior):
+    """Algorithmic bytes of one whole step: interior_bytes per interior cell
+    (read p^n, read p^{n-1}, write p^{n+1}); per boundary point 4 B of index
+    plus, per filter face, 8 K B of filter history read and 8 B of state
+    written; 32 B per PML cell (auxiliary fields and psi read and written)."""
+    K = info.ncoef
+    faces = [1] * 6 + [2] * 12 + [3] * 8
+    lrs = sum(int(info.group_counts[g]) * (4 + 8 * K * faces[g] + 8 * faces[g]) for g in range(26))
+    pml = 32 * int(info.n_pml_cells)
+    parts = {"interior": interior_bytes * interior, "boundary": lrs, "pml": pml}
+    return float(sum(parts.values())), parts
+
+
+PARITY_STEPS = 240
+
+
+def parity_leg(make_sim, cfg, info, f16):
+    """The error of this line's own configuration: the benchmark workload run
+    again for PARITY_STEPS steps with the timed run's streaming plan, against
+    the CPU restatement of the same scheme in FP32 (bit for bit expected) and
+    in FP64 (receivers and the whole field; the receivers farther than
+    PARITY_STEPS * lambda cells from the source are still silent)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    sim = make_sim()
+    sim.set_plan(per_sm=info.stream_per_sm, dz=info.tile_z, beside=bool(info.stream_beside))
+    sim.Run(PARITY_STEPS)
+    got, field = sim.mics(), sim.field()
+    sim.close()
+    src = [(cfg.sources[0][0], cfg.sources[0][1][:PARITY_STEPS])]
+    kw = dict(dx=cfg.dx, c=cfg.c, dt=cfg.dt, mode=1, pml_width=cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi,
+              sources=src, receivers=cfg.receivers, steps=PARITY_STEPS, want_field=True)
+    a, b = cfg.a.astype(np.float32), cfg.b.astype(np.float32)
+    w32, f32 = oracle.simulate(cfg.dims, cfg.vox, a, b, precision="f16" if f16 else "f32", **kw)
+    w64, f64 = oracle.simulate(cfg.dims, cfg.vox, a, b, precision="f64", **kw)
+
+    def rl(x, y):
+        return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30))
+    live = np.abs(w64).max(axis=1) > 0
+    return {"steps": PARITY_STEPS, "plan": [info.stream_per_sm, info.tile_z, bool(info.stream_beside)],
+            "oracle": "fp16-storage restatement" if f16 else "fp32 restatement",
+            "receivers_bitexact": bool(np.array_equal(got, w32)), "field_bitexact": bool(np.array_equal(field, f32)),
+            "receiver_rel_l2_vs_oracle": rl(got, w32), "receiver_rel_l2_vs_fp64": rl(got[live], w64[live]),
+            "field_rel_l2_vs_fp64": rl(field, f64), "receivers_with_signal": int(live.sum())}
 
 
 def timeline_leg(sim):
@@ -609,8 +730,9 @@ def e2e_leg(sim, cfg, K, interior, world, metric):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# dominant kernel, measured with ncu on the full-size workload
-# (profiles/k_stream_dram_512x384x320_fp32.md), keyed by grid and storage.
+# dominant kernel, from one ncu capture of that kernel on the full-size
+# workload (the ncu summary in profiles/ records the command), keyed by grid
+# and storage; the line reports it with traffic_source "ncu capture".
 MEASURED_TRAFFIC = {((512, 384, 320), "fp32"): ("interior_stream", 740.42e6)}
 
 
@@ -634,6 +756,8 @@ def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0, traffic_key=None):
         traffic = known[1]
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+            "traffic_source": "ncu capture of one full-size launch of this kernel (not measured by this run)"
+            if traffic else None,
             "bytes_per_launch": step_kernel_bytes, "avg_launch_ms": avg_ms,
             "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in stats.items() if v[0]}}
 

@@ -137,8 +137,10 @@ int afd_model_boundary(const afd_model* m, int32_t device, int32_t* out, int64_t
 const char* afd_model_last_error(const afd_model* m);
 void afd_model_destroy(afd_model* m);
 
-/* FP64 admittance-filter check (run on the GPU when one is present, else
- * on the host): stability = every root of b(z) (the recursion's
+/* FP64 admittance-filter check, a coefficient check made once before a
+ * run (not part of the step): on the GPU when one is present; without a CUDA
+ * device the same FP64 arithmetic runs on the host, so that models can be
+ * checked on machines without a GPU. Stability = every root of b(z) (the recursion's
  * denominator, coefficient order b0 + b1 z^-1 + ...) inside |z| < 1 - margin;
  * passivity = Re{A(e^jw)/B(e^jw)} >= 0 on n_freq uniformly spaced
  * frequencies in [0, pi]. status[i] bit0 = unstable, bit1 = not passive.
@@ -148,15 +150,18 @@ int afd_check_filters(int32_t nmat, int32_t ncoef, const double* a, const double
 
 /* No counterpart in the reference. The same check as afd_check_filters for
  * callers that must not allocate device memory (a process held to a fixed
- * GPU memory budget by its host application, or a control thread that
- * re-checks coefficients while simulations run and may not grow the device
- * heap): its scratch is one file-scope device array of 64 materials x 16
- * coefficients (about 21 KB, held by every device that loads the library
- * until exit). Sizes beyond that return AFD_ERR_ARG. Needs a CUDA device.
- * The first call on a device looks up the array's address with that device
- * current; make it before any stream capture. All calls share the array:
- * calls that overlap on the GPU race, so the caller serialises them. The
- * error text is afd_model_last_error(NULL). */
+ * GPU memory budget by its host application, or a setup path that re-checks
+ * coefficients after simulations have taken the rest of the device, where a
+ * cudaMalloc could fail): its scratch is one file-scope device array of 64
+ * materials x 16 coefficients (about 21 KB, held by every device that loads
+ * the library until exit). Sizes beyond that return AFD_ERR_ARG. Needs a
+ * CUDA device. Each call looks up the array's address with the device
+ * current (valid after a cudaDeviceReset too); the first call on a device
+ * loads the module there, so make it before any stream capture. The copies
+ * are synchronous and the kernels run on the legacy default stream: a call
+ * waits for work on the device's blocking streams. All calls share the
+ * array: calls that overlap on the GPU race, so the caller serialises them.
+ * The error text is afd_model_last_error(NULL). */
 int afd_check_filters_static(int32_t nmat, int32_t ncoef, const double* a, const double* b,
                              int32_t n_freq, int32_t* status, double* min_real, double* max_root);
 
@@ -287,7 +292,8 @@ typedef struct afd_info {
     int32_t stream_blocks;       /* resident blocks of the streaming kernel's plan */
     int32_t tuned;               /* 1 once the online autotuner has chosen the plan */
     int32_t stream_beside;       /* 1: the plan runs the boundary and PML kernels beside the streaming kernel */
-    int32_t reserved[6];
+    int32_t stream_per_sm;       /* resident streaming blocks per SM of the plan */
+    int32_t reserved[5];
 } afd_info;
 int afd_get_info(afd_sim* s, afd_info* info);
 
@@ -304,6 +310,26 @@ int afd_energy(afd_sim* s, int32_t batch, double* energy);
  * passed as void*), e.g. so that the caller can bracket afd_run with its own
  * CUDA events. NULL restores the library's own stream. */
 int afd_set_stream(afd_sim* s, void* stream);
+
+/* A streaming-kernel plan (the autotuner's search space). Zero fields take
+ * the default: the 64x16 tile, as many resident blocks per SM as fit, the
+ * z-chunk depth rule. beside = 1 runs the boundary and PML pressure kernels
+ * beside the streaming kernel, which then skips their cells (FIXED scheme
+ * with CUDA graphs only; ignored elsewhere). */
+typedef struct afd_plan {
+    int32_t tile_x, tile_y;  /* streaming tile in cells: 64x16, 128x8 or 32x32 (FP16 storage doubles x) */
+    int32_t per_sm;          /* resident streaming blocks per SM */
+    int32_t dz;              /* planes per z-chunk work item (1..1024) */
+    int32_t beside;
+    int32_t reserved[3];
+} afd_plan;
+
+/* Fixes the streaming plan of later runs and turns the online autotuner off
+ * for this simulation (no counterpart in the reference, whose kernels have
+ * one launch shape: clh-kernel.hpp:163-183). NULL gives the plan back to the
+ * autotuner, which tries its candidates again. Every plan gives the same
+ * results bit for bit. */
+int afd_set_plan(afd_sim* s, const afd_plan* plan);
 
 /* Per-kernel statistics of the last afd_run made with params.profile set:
  * kernel idx (0-based) -> name, launches and summed device milliseconds.

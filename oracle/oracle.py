@@ -45,6 +45,19 @@ def _fn(impl, precision):
     return fn
 
 
+def ref_timing(pml_parallel, precision="f32"):
+    """Timing controls of the reference harness (impl "ref"): whether its PML
+    NDRange runs over all host threads (as a CPU OpenCL device runs it) and a
+    reader of the last call's step-loop wall seconds (set-up excluded)."""
+    lib = C.CDLL(REF_LIBS[precision])
+    lib.ref_set_pml_parallel.argtypes = [C.c_int]
+    lib.ref_set_pml_parallel.restype = None
+    lib.ref_last_loop_seconds.argtypes = []
+    lib.ref_last_loop_seconds.restype = C.c_double
+    lib.ref_set_pml_parallel(1 if pml_parallel else 0)
+    return lib.ref_last_loop_seconds
+
+
 def _p(a, t):
     return a.ctypes.data_as(P(t))
 

@@ -20,8 +20,13 @@
  * Work-items of leapfrog and of the boundary kernels are independent and
  * run in parallel; the PML kernel writes cells that other work-items read
  * (pml.cl:188 vs :124-137), so it runs its NDRange serially in x-fastest
- * order, one legal schedule of the kernel.
+ * order, one legal schedule of the kernel. For timing only,
+ * ref_set_pml_parallel(1) runs that NDRange over all host threads the way a
+ * CPU OpenCL device would (its results then depend on the schedule, as the
+ * reference's do on a device); ref_last_loop_seconds() gives the wall time
+ * of the last call's step loop, set-up excluded.
  */
+#include <omp.h>
 #include <stddef.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -245,6 +250,12 @@ static const lrs_fn kLrs[26] = {
 #define REF_NAME ref_simulate_f32
 #endif
 
+static int g_pml_parallel = 0;
+static double g_loop_seconds = 0.0;
+
+void ref_set_pml_parallel(int on) { g_pml_parallel = on != 0; }
+double ref_last_loop_seconds(void) { return g_loop_seconds; }
+
 /*
  * Same arguments as the oracle restatement's ora_simulate_*; mode must be 0
  * (the reference has only its own semantics) and faces is ignored.
@@ -324,6 +335,7 @@ int REF_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
     g_gsz[2] = (size_t)nz;
 
     unsigned ix_buf = 0, sim_cnt = 0;
+    const double t_loop = omp_get_wtime();
     for (int r = 0; r < n_runs; ++r) {
         for (int64_t i = 0; i < run_steps[r]; ++i) {
             { float* t0 = P[2]; P[2] = P[1]; P[1] = P[0]; P[0] = t0; } /* rotate(begin, begin+2) */
@@ -355,6 +367,7 @@ int REF_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
                 for (int ax = 0; ax < 3; ++ax) { float* t0 = fi[ax][0]; fi[ax][0] = fi[ax][1]; fi[ax][1] = t0; }
                 { float* t0 = psi[0]; psi[0] = psi[1]; psi[1] = t0; }
                 g_gsz[0] = (size_t)nx; g_gsz[1] = (size_t)ny; g_gsz[2] = (size_t)nz;
+#pragma omp parallel for schedule(static) if (g_pml_parallel)
                 for (int z = 0; z < nz; ++z)
                     for (int y = 0; y < ny; ++y)
                         for (int x = 0; x < nx; ++x) {
@@ -384,6 +397,7 @@ int REF_NAME(int mode, int nx, int ny, int nz, int mx, int my, int mz, const int
         }
         sim_cnt += (unsigned)run_steps[r];
     }
+    g_loop_seconds = omp_get_wtime() - t_loop;
     for (int m = 0; m < nrcv; ++m)
         for (int64_t t = 0; t < total; ++t) rcv_out[(size_t)m * total + t] = (f32)mic_rec[(size_t)m * total + t];
     if (field_out)

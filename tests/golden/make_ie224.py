@@ -33,7 +33,7 @@ def load_pkg():
     return mod
 
 
-def main(ref=sys.argv[1] if len(sys.argv) > 1 else "/root/reference"):
+def main(ref=sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ANC_FIELD_REFERENCE", "/root/reference")):
     pkg = load_pkg()
     m = pkg.Model.load_kerkythea(os.path.join(ref, "examples", "models", "ie224", "model.xml"), 0.02)
     vox = m.voxels().ravel()

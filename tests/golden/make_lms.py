@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/anc_field_py/ancutil.py"
+REF = os.path.join(os.environ.get("ANC_FIELD_REFERENCE", "/root/reference"), "anc_field_py", "ancutil.py")
 
 # (name, input length, output length, taps, mu, seed, kind)
 CASES = [("fir4", 400, 400, 16, 1e-3, 1, "white"), ("odd", 257, 257, 33, 5e-3, 2, "white"),

@@ -91,7 +91,7 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def main(ref=sys.argv[1] if len(sys.argv) > 1 else "/root/reference"):
+def main(ref=sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ANC_FIELD_REFERENCE", "/root/reference")):
     pkg = load_pkg()
     mdir = os.path.join(ref, "examples", "models")
     out = {}

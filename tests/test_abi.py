@@ -12,7 +12,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "afd.h")
-REFERENCE_MODELS = "/root/reference/examples/models"
+# the reference tree, when present on this machine (the shipped-model checks
+# skip without it); the oracle's build recipe reads the same variable
+REFERENCE_MODELS = os.path.join(os.environ.get("ANC_FIELD_REFERENCE", "/root/reference"), "examples", "models")
 
 
 def declared_functions():
@@ -289,7 +291,7 @@ def test_device_kerkythea_loader_reports_missing_device_or_bad_file(pkg, tmp_pat
 
 
 def test_ctypes_structs_match_the_header(pkg, tmp_path):
-    """sizeof and every field offset of afd_params, afd_info and
+    """sizeof and every field offset of afd_params, afd_info, afd_plan and
     afd_mlp_params as the C compiler lays them out from include/, against
     the ctypes mirrors."""
     import shutil
@@ -297,7 +299,8 @@ def test_ctypes_structs_match_the_header(pkg, tmp_path):
     cc = shutil.which("gcc") or shutil.which("cc")
     if cc is None:
         pytest.skip("no C compiler")
-    structs = {"afd_params": pkg.afd.Params, "afd_info": pkg.afd.Info, "afd_mlp_params": pkg.surrogate.MlpParams}
+    structs = {"afd_params": pkg.afd.Params, "afd_info": pkg.afd.Info, "afd_plan": pkg.afd.Plan,
+               "afd_mlp_params": pkg.surrogate.MlpParams}
     lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "afd.h"', '#include "afd_surrogate.h"',
              "int main(void) {"]
     for cname, py in structs.items():

@@ -1,7 +1,8 @@
 """The streaming plan's online autotuner and the FIXED-scheme launch order
 with the boundary and PML kernels beside the streaming kernel: a run long
-enough to try every candidate plan (and switch plans between chunks)
-equals the serial run without graphs bit for bit, in FP32 and FP16."""
+enough to try every candidate plan (and switch plans, tile shapes among
+them, between chunks) equals the serial run without graphs bit for bit, in
+FP32 and FP16."""
 import numpy as np
 import pytest
 
@@ -18,7 +19,7 @@ def test_tuned_run_equals_serial_run(pkg, storage):
     vox = W.close_gaps(vox)
     nz, ny, nx = vox.shape
     ksi = W.ksi_arrays((nx, ny, nz), 8, W.FACE_ZP, kmax=6000.0)
-    sig = W.gaussian_pulse(1400, 32000.0)
+    sig = W.gaussian_pulse(2400, 32000.0)
     out = []
     for graphs in (1, 0):
         sim = pkg.Simulation(mode=1, graphs=graphs, storage=storage)
@@ -27,7 +28,7 @@ def test_tuned_run_equals_serial_run(pkg, storage):
         sim.AddSourceCell((30, 30, 20), sig)
         for r in [(50, 40, 30), (80, 20, 55), (10, 60, 10)]:
             sim.AddMicCell(r)
-        sim.Run(1201)
+        sim.Run(2201)
         sim.Run(199)
         info = sim.info()
         assert bool(info.tuned) == bool(graphs)
@@ -44,7 +45,7 @@ def test_tuned_batch_equals_serial_run(pkg, storage):
     half-depth candidate too, and a tuned run that tries every candidate
     equals the serial run without graphs bit for bit, member by member."""
     W = pkg.workloads
-    cfg = W.config_c3(steps=1400)
+    cfg = W.config_c3(steps=2200)
     out = []
     for graphs in (1, 0):
         sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, batch=16, graphs=graphs, storage=storage)
@@ -55,8 +56,51 @@ def test_tuned_batch_equals_serial_run(pkg, storage):
                 sim.AddSourceCell(cell, sig, batch=m)
         for r in cfg.receivers:
             sim.AddMicCell(r)
-        sim.Run(1400)
+        sim.Run(2200)
         assert bool(sim.info().tuned) == bool(graphs)
         out.append(np.stack([sim.mics(batch=m) for m in range(16)]))
         sim.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_every_plan_twice_equals_serial_run(pkg, storage):
+    """Every streaming plan, forced with afd_set_plan and run twice from the
+    start, equals the serial run without graphs bit for bit (a result that
+    changed between two runs of one plan would be a race): all resident
+    blocks or one fewer, the rule's z-chunk depth or a quarter of it, and the
+    boundary/PML pressure kernels beside the streaming kernel, on the
+    16-member secondary-path batch (FP16 storage keeps a scale per member)."""
+    W = pkg.workloads
+    cfg = W.config_c3(steps=600)
+
+    def run(graphs, plan=None):
+        sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, batch=16, graphs=graphs, storage=storage)
+        sim.SetModel(pkg.Model.from_voxels(cfg.vox, cfg.a.astype(np.float32), cfg.b.astype(np.float32)))
+        sim.SetPml(cfg.pml_width, faces=cfg.pml_faces, ksi=cfg.ksi)
+        if plan is not None:
+            sim.set_plan(**plan)
+        for m in range(16):
+            for cell, sig in cfg.batch_sources[m]:
+                sim.AddSourceCell(cell, sig, batch=m)
+        for r in cfg.receivers:
+            sim.AddMicCell(r)
+        sim.Run(600)
+        info = sim.info()
+        if plan is not None:
+            assert bool(info.stream_beside) == plan.get("beside", False)
+            assert (info.tile_x, info.tile_y) == plan.get("tile", (64 * (2 if storage else 1), 16))
+        out = np.stack([sim.mics(batch=m) for m in range(16)]), sim.field(batch=7)
+        sim.close()
+        return out
+
+    serial = run(0)
+    wide = 2 if storage else 1  # FP16 storage doubles the tile width in cells
+    plans = [dict(), dict(dz=8), dict(beside=True), dict(beside=True, per_sm=1), dict(tile=(32 * wide, 32))]
+    if not storage:
+        plans.append(dict(tile=(128, 8), dz=8))
+    for plan in plans:
+        for _ in range(2):
+            got = run(1, plan)
+            assert np.array_equal(got[0], serial[0]), plan
+            assert np.array_equal(got[1], serial[1]), plan

@@ -1,7 +1,9 @@
 """afd_check_filters_static: the filter check for callers that may not
 allocate device memory (its scratch is a fixed device array inside the
 library). Through the C ABI it must return what afd_check_filters returns,
-call after call, even though every call reuses the same scratch.
+call after call, even though every call reuses the same scratch; it must
+agree with numpy's roots and admittance; and it must work when no device
+memory is left to allocate.
 
 This file is collected last so that a run that stops at the first failure
 has already run every other test; it also passes when run alone.
@@ -69,3 +71,88 @@ def test_static_rejects_sizes_beyond_its_scratch(pkg):
     assert rc0 == rc1 == 0
     assert np.array_equal(st0, st1)
     np.testing.assert_allclose(mr1, mr0, rtol=RTOL, atol=0.0)
+
+
+def test_static_against_independent_restatement(pkg):
+    """Stability radius against numpy's polynomial roots and the passivity
+    minimum against the numpy admittance on the same frequency grid, on the
+    GPU box (the CPU suite checks the host path the same way)."""
+    import ancfield_b200.workloads as W
+    lib = pkg.afd.library()
+    a, b = _filters(14)
+    rc, st, mr, rt = _call(lib, "afd_check_filters_static", a, b)
+    assert rc == 0
+    np.testing.assert_allclose(rt, [np.abs(np.roots(b[m])).max() for m in range(len(b))], rtol=1e-9)
+    np.testing.assert_allclose(mr, W.admittance_real_min(a, b), rtol=1e-9)
+
+
+def test_static_full_layout_and_coefficient_limit(pkg):
+    """64 materials x 16 coefficients (the b, root and partial-minimum slots
+    at their largest offsets) equals the allocating check; 17 coefficients
+    are rejected before anything runs."""
+    import ancfield_b200.workloads as W
+    lib = pkg.afd.library()
+    a, b = W.passive_filters(64, 16, 15)
+    rc0, st0, mr0, rt0 = _call(lib, "afd_check_filters", a, b)
+    rc1, st1, mr1, rt1 = _call(lib, "afd_check_filters_static", a, b)
+    assert rc0 == 0 and rc1 == 0
+    assert np.array_equal(st0, st1) and not st1.any()
+    np.testing.assert_allclose(mr1, mr0, rtol=RTOL, atol=0.0)
+    np.testing.assert_allclose(rt1, rt0, rtol=RTOL, atol=0.0)
+    rc, _, _, _ = _call(lib, "afd_check_filters_static", np.ones((4, 17)), np.ones((4, 17)))
+    assert rc == pkg.afd.ERR_ARG
+
+
+def _cudart():
+    """The CUDA runtime as a plain C library (the device allocations below go
+    down to 512 bytes, finer than torch's 2 MB segments)."""
+    import glob
+    import os
+    import nvidia.cuda_runtime as rt
+    for path in sorted(glob.glob(os.path.join(list(rt.__path__)[0], "lib", "libcudart.so*"))) + [
+            "libcudart.so.12", "libcudart.so"]:
+        try:
+            lib = C.CDLL(path)
+            lib.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+            lib.cudaFree.argtypes = [C.c_void_p]
+            return lib
+        except OSError:
+            continue
+    pytest.skip("no CUDA runtime library to allocate with")
+
+
+def test_static_runs_with_no_device_memory_left(pkg):
+    """The property itself: with every byte of device memory that can be
+    allocated taken, the allocating check fails to allocate while the static
+    one still returns its usual answer."""
+    import torch
+    lib = pkg.afd.library()
+    a, b = _filters(16)
+    rc, st_ref, mr_ref, _ = _call(lib, "afd_check_filters_static", a, b)  # module loaded, address looked up
+    assert rc == 0
+    rt = _cudart()
+    torch.cuda.synchronize()
+    hold, raw = [], []
+    try:
+        while True:
+            try:
+                hold.append(torch.empty(1 << 30, dtype=torch.uint8, device="cuda"))
+            except torch.OutOfMemoryError:
+                break
+        for chunk in (1 << 26, 1 << 21, 1 << 16, 1 << 12, 512):
+            while len(raw) < 100000:
+                p = C.c_void_p()
+                if rt.cudaMalloc(C.byref(p), chunk) != 0:
+                    break
+                raw.append(p)
+        rc0, _, _, _ = _call(lib, "afd_check_filters", a, b)
+        rc1, st1, mr1, _ = _call(lib, "afd_check_filters_static", a, b)
+    finally:
+        for p in raw:
+            rt.cudaFree(p)
+        hold.clear()
+        torch.cuda.empty_cache()
+    assert rc0 == pkg.afd.ERR_CUDA
+    assert rc1 == 0
+    assert np.array_equal(st1, st_ref)
+    np.testing.assert_allclose(mr1, mr_ref, rtol=RTOL, atol=0.0)
