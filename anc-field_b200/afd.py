@@ -39,7 +39,8 @@ EXPORTS = [
     "afd_add_receiver_cell", "afd_run", "afd_prepare", "afd_get_receivers", "afd_update_source",
     "afd_get_receivers_range", "afd_get_field", "afd_get_plane", "afd_set_capture", "afd_get_frames",
     "afd_set_timeline", "afd_get_timeline", "afd_wait_selftest",
-    "afd_get_info", "afd_energy", "afd_set_stream", "afd_set_plan", "afd_kernel_stats", "afd_last_error",
+    "afd_get_info", "afd_energy", "afd_set_stream", "afd_set_plan", "afd_set_slab", "afd_step_phase", "afd_halo",
+    "afd_kernel_stats", "afd_last_error",
     "afd_destroy",
 ]
 
@@ -133,6 +134,9 @@ def library(path=LIB_PATH):
         "afd_energy": (C.c_int, [vp, i32, P(f64)]),
         "afd_set_stream": (C.c_int, [vp, vp]),
         "afd_set_plan": (C.c_int, [vp, P(Plan)]),
+        "afd_set_slab": (C.c_int, [vp, i32, i32]),
+        "afd_step_phase": (C.c_int, [vp, i32]),
+        "afd_halo": (C.c_int, [vp, i32, i32, i32, vp, i64]),
         "afd_kernel_stats": (C.c_int, [vp, i32, C.c_char_p, i64, P(i64), P(f64)]),
         "afd_last_error": (C.c_char_p, [vp]),
         "afd_destroy": (None, [vp]),
@@ -455,6 +459,23 @@ class Simulation:
             return
         p = Plan(tile[0], tile[1], per_sm, dz, 1 if beside else 0)
         self._check(library().afd_set_plan(self._h, C.byref(p)))
+
+    # --- z-slab decomposition ----------------------------------------
+    def set_slab(self, z_offset, nz_global):
+        """This grid is global planes z_offset.. of nz_global planes; its end
+        planes are halos filled between step phases (nz_global 0: off)."""
+        self._check(library().afd_set_slab(self._h, z_offset, nz_global))
+
+    def step_phase(self, phase):
+        """Phase 1 (interior, boundary, PML pressure) or phase 2 (PML
+        auxiliary fields, sources, receivers) of the next step."""
+        self._check(library().afd_step_phase(self._h, phase))
+
+    def halo(self, side, direction, field, dev_ptr, cap):
+        """Plane copy between the simulation and a device buffer (afd_halo):
+        side 0/1 low/high z, direction 0 read own plane / 1 write halo,
+        field 0 pressure, 1..3 auxiliary x/y/z, 4 psi."""
+        self._check(library().afd_halo(self._h, side, direction, field, C.c_void_p(dev_ptr), cap))
 
     def kernel_stats(self):
         L = library()

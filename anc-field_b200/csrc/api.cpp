@@ -410,6 +410,16 @@ int afd_set_stream(afd_sim* s, void* stream) { SIM_CALL(s, s->eng->set_stream(st
 
 int afd_set_plan(afd_sim* s, const afd_plan* plan) { SIM_CALL(s, s->eng->set_plan(plan)); }
 
+int afd_set_slab(afd_sim* s, int32_t z_offset, int32_t nz_global) {
+    SIM_CALL(s, s->eng->set_slab(z_offset, nz_global));
+}
+
+int afd_step_phase(afd_sim* s, int32_t phase) { SIM_CALL(s, s->eng->step(phase)); }
+
+int afd_halo(afd_sim* s, int32_t side, int32_t dir, int32_t field, void* dev, int64_t cap) {
+    SIM_CALL(s, s->eng->halo(side, dir, field, dev, cap));
+}
+
 int afd_kernel_stats(afd_sim* s, int32_t idx, char* name, int64_t cap, int64_t* launches, double* ms) {
     if (!s) return AFD_ERR_ARG;
     return s->eng->kernel_stats(idx, name, cap, launches, ms);

@@ -63,6 +63,9 @@ struct PmlDev {
     int64_t n_units;
     const uint32_t* cells;
     int32_t words_per_row;
+    // z-slab of a larger grid: local plane z is global plane z + zoff of
+    // nz_glob planes; the PML cell rule and the z slabs use global planes
+    int32_t zoff, nz_glob;
 };
 
 struct SrcDev {

@@ -348,7 +348,8 @@ __device__ __forceinline__ unsigned slab_axes(const StepArgs& a, int x0, int x1,
     unsigned ax = 0;
     if (((F & AFD_FACE_XM) && x0 < W) || ((F & AFD_FACE_XP) && x1 > a.g.nx - W - 1)) ax |= 1u;
     if (((F & AFD_FACE_YM) && y0 < W) || ((F & AFD_FACE_YP) && y1 > a.g.ny - W - 1)) ax |= 2u;
-    if (((F & AFD_FACE_ZM) && z0 < W) || ((F & AFD_FACE_ZP) && z1 > a.g.nz - W - 1)) ax |= 4u;
+    const int zg0 = z0 + a.pml.zoff, zg1 = z1 + a.pml.zoff;
+    if (((F & AFD_FACE_ZM) && zg0 < W) || ((F & AFD_FACE_ZP) && zg1 > a.pml.nz_glob - W - 1)) ax |= 4u;
     return ax;
 }
 
@@ -357,19 +358,6 @@ __device__ __forceinline__ unsigned slab_axes(const StepArgs& a, int x0, int x1,
 __device__ __forceinline__ unsigned pml_mask4(const StepArgs& a, int x, int y, int z) {
     const PmlDev& P = a.pml;
     return (__ldg(P.cells + ((int64_t)z * a.g.ny + y) * P.words_per_row + (x >> 5)) >> (x & 31)) & 15u;
-}
-
-// Thread -> (batch member, first cell) of a box launch: x in 4-cell units,
-// rows in y, planes (times batch members) in z.
-__device__ __forceinline__ bool box_cell(const PmlBox& bx, int& b, int& x, int& y, int& z) {
-    const int ux = blockIdx.x * blockDim.x + threadIdx.x;
-    const int yy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ux >= bx.units || yy >= bx.height) return false;
-    b = (int)(blockIdx.z / (unsigned)bx.depth);
-    z = bx.z0 + (int)(blockIdx.z % (unsigned)bx.depth);
-    x = bx.x0 + 4 * ux;
-    y = bx.y0 + yy;
-    return true;
 }
 
 // Values x..x+4 of a row (x a multiple of 4). hi = false: the fifth value
@@ -432,33 +420,22 @@ __device__ __forceinline__ void store4t(T* p, const float v[4], unsigned m, floa
 }
 
 // Pressure of the PML cells (pml.cl:185-207 restricted to the slab cells)
-// over one box of the disjoint box cover, four consecutive cells per
-// thread. Fields outside the read axes are identically zero there and are
-// not loaded; PSI: psi is kept (PML faces on all three axes). Four blocks
-// per SM (64 registers, no spills in any variant): the FP16 build would
-// otherwise take 79 registers and three blocks.
+// of one 4-cell unit x..x+3 of row (y, z). Fields outside the read axes are
+// identically zero there and are not loaded; PSI: psi is kept (PML faces on
+// all three axes). s_new, ic, io: FP16 scales of the new level and inverse
+// scales of p^n and p^{n-1} (1 for FP32 storage).
 template <bool PSI, typename T>
-__global__ void __launch_bounds__(256, 4) k_pml_box_p(const __grid_constant__ StepArgs a, const PmlBox bx, int j) {
-    int b, x, y, z;
-    if (!box_cell(bx, b, x, y, z)) return;
+__device__ __forceinline__ void pml_p_unit(const StepArgs& a, int b, int x, int y, int z, long long g,
+                                           float s_new, float ic, float io) {
     const unsigned m = pml_mask4(a, x, y, z);
     if (!m) return;
     const PmlDev& P = a.pml;
-    const long long g = *a.d_step + j;
-    const TlMark tl(a, 2, g, blockIdx.z < (unsigned)bx.depth);
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
     const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
     const T* pc = level_ptr<T>(a, buf_cur(g)) + base;
     const T* po = level_ptr<T>(a, buf_old(g)) + base;
     T* pn = level_ptr<T>(a, buf_new(g)) + base;
-    float s_new = 1.0f, ic = 1.0f, io = 1.0f;
-    if constexpr (sizeof(T) == 2) {
-        const StepScales sc = step_scales(a.f16, b, g);
-        s_new = sc.s_new;
-        ic = sc.inv_cur;
-        io = sc.inv_old;
-    }
     const int lv = pml_level(a, g);
     // x+4 is read only for the unit's last cell, x-1 only for its first
     const bool hi = (m & 8u) != 0;
@@ -565,31 +542,22 @@ __global__ void __launch_bounds__(256, 4) k_pml_box_p(const __grid_constant__ St
     store4t(pn + i, v, m, s_new);
 }
 
-// Auxiliary field AX of the PML cells of one slab box (pml.cl:231-262 with
-// the derivative and ksi index corrected). The derivatives of the new and
-// previous pressure along every axis come from the same four rows
-// (y, y+1) x (z, z+1), x..x+4.
+// Auxiliary field AX of the PML cells of one 4-cell unit (pml.cl:231-262
+// with the derivative and ksi index corrected). The derivatives of the new
+// and previous pressure along every axis come from the same four rows
+// (y, y+1) x (z, z+1), x..x+4. in_, ic: FP16 inverse scales of the new
+// level and of p^n (1 for FP32 storage).
 template <int AX, bool PSI, typename T>
-__global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ StepArgs a, const PmlBox bx,
-                                                     int j) {
-    const TlMark tl(a, 3 + AX, *a.d_step + j, blockIdx.z < (unsigned)bx.depth);
-    int b, x, y, z;
-    if (!box_cell(bx, b, x, y, z)) return;
+__device__ __forceinline__ void pml_aux_unit(const StepArgs& a, int b, int x, int y, int z, long long g,
+                                             float in_, float ic) {
     const unsigned m = pml_mask4(a, x, y, z);
     if (!m) return;
     const PmlDev& P = a.pml;
-    const long long g = *a.d_step + j;
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
     const int64_t i = (int64_t)z * plane + (int64_t)y * pitch + x;
     const T* pn = level_ptr<T>(a, buf_new(g)) + base + i;
     const T* pc = level_ptr<T>(a, buf_cur(g)) + base + i;
-    float in_ = 1.0f, ic = 1.0f;
-    if constexpr (sizeof(T) == 2) {
-        const StepScales sc = step_scales(a.f16, b, g);
-        in_ = sc.inv_new;
-        ic = sc.inv_cur;
-    }
     const int lv = pml_level(a, g);
     const bool hi = (m & 8u) != 0;  // x+4 is read only for the unit's last cell
     float n00[5], n01[5], n10[5], n11[5], m00[5], m01[5], m10[5], m11[5];
@@ -665,6 +633,97 @@ __global__ void __launch_bounds__(256) k_pml_box_aux(const __grid_constant__ Ste
         }
     }
     store4(P.fi[AX][lv] + base + i, out, m);
+}
+
+// One launch over several PML boxes: a flat grid whose blocks are dealt to
+// the boxes in order (start[k] .. start[k+1]-1 to entry k). Within an entry
+// a block holds w units across (w = min(units, 32)) and 256 / w rows, and
+// every thread marches zc planes of its column; the planes (times the batch
+// members) are split into chunks of zc.
+constexpr int kMaxLaunchBoxes = 9;
+struct BoxLaunch {
+    int32_t n, zc;
+    PmlBox box[kMaxLaunchBoxes];
+    int32_t axis[kMaxLaunchBoxes];  // auxiliary launches: the field of the entry
+    int32_t w[kMaxLaunchBoxes], gx[kMaxLaunchBoxes], gy[kMaxLaunchBoxes], gzc[kMaxLaunchBoxes];
+    int32_t start[kMaxLaunchBoxes + 1];
+};
+
+struct BoxThread {
+    int k, b, x, y, z0, z1;
+    bool ok;
+};
+
+__device__ __forceinline__ BoxThread box_thread(const BoxLaunch& L) {
+    BoxThread t;
+    int k = 0;
+    while (k + 1 < L.n && (int)blockIdx.x >= L.start[k + 1]) ++k;
+    t.k = k;
+    const PmlBox& bx = L.box[k];
+    const int w = L.w[k], rows = 256 / w;
+    int r = (int)blockIdx.x - L.start[k];
+    const int bxi = r % L.gx[k];
+    r /= L.gx[k];
+    const int byi = r % L.gy[k];
+    r /= L.gy[k];
+    const int zci = r % L.gzc[k];
+    t.b = r / L.gzc[k];
+    const int ux = bxi * w + (int)threadIdx.x % w, yy = byi * rows + (int)threadIdx.x / w;
+    t.ok = (int)threadIdx.x < w * rows && ux < bx.units && yy < bx.height;
+    t.x = bx.x0 + 4 * ux;
+    t.y = bx.y0 + yy;
+    t.z0 = bx.z0 + zci * L.zc;
+    t.z1 = min(t.z0 + L.zc, bx.z0 + bx.depth);
+    return t;
+}
+
+// PML pressure over every box of the disjoint box cover in one launch. Four
+// blocks per SM (64 registers in every variant).
+template <bool PSI, typename T>
+__global__ void __launch_bounds__(256, 3) k_pml_p_all(const __grid_constant__ StepArgs a,
+                                                      const __grid_constant__ BoxLaunch L, int j) {
+    const long long g = *a.d_step + j;
+    const BoxThread t = box_thread(L);
+    const TlMark tl(a, 2, g, t.b == 0);
+    if (!t.ok) return;
+    float s_new = 1.0f, ic = 1.0f, io = 1.0f;
+    if constexpr (sizeof(T) == 2) {
+        const StepScales sc = step_scales(a.f16, t.b, g);
+        s_new = sc.s_new;
+        ic = sc.inv_cur;
+        io = sc.inv_old;
+    }
+#pragma unroll 1
+    for (int z = t.z0; z < t.z1; ++z) pml_p_unit<PSI, T>(a, t.b, t.x, t.y, z, g, s_new, ic, io);
+}
+
+// The auxiliary fields of every (axis, slab box) pair in one launch: the
+// fields are disjoint outputs and read only the new pressure, p^n, the new
+// psi and their own previous level.
+template <bool PSI, typename T>
+__global__ void __launch_bounds__(256, 3) k_pml_aux_all(const __grid_constant__ StepArgs a,
+                                                        const __grid_constant__ BoxLaunch L, int j) {
+    const long long g = *a.d_step + j;
+    const BoxThread t = box_thread(L);
+    const int ax = L.axis[t.k];
+    const TlMark tl(a, 3 + ax, g, t.b == 0);
+    if (!t.ok) return;
+    float in_ = 1.0f, ic = 1.0f;
+    if constexpr (sizeof(T) == 2) {
+        const StepScales sc = step_scales(a.f16, t.b, g);
+        in_ = sc.inv_new;
+        ic = sc.inv_cur;
+    }
+    if (ax == 0) {
+#pragma unroll 1
+        for (int z = t.z0; z < t.z1; ++z) pml_aux_unit<0, PSI, T>(a, t.b, t.x, t.y, z, g, in_, ic);
+    } else if (ax == 1) {
+#pragma unroll 1
+        for (int z = t.z0; z < t.z1; ++z) pml_aux_unit<1, PSI, T>(a, t.b, t.x, t.y, z, g, in_, ic);
+    } else {
+#pragma unroll 1
+        for (int z = t.z0; z < t.z1; ++z) pml_aux_unit<2, PSI, T>(a, t.b, t.x, t.y, z, g, in_, ic);
+    }
 }
 
 // Eight binary16 values (one 16-byte word) as FP32 numbers.
@@ -1237,6 +1296,16 @@ struct Engine::Impl {
     DBuf<float> ksi_dev[3];
     std::vector<PmlBox> pml_boxes;
     std::vector<PmlBox> pml_axis_boxes[3];
+    // the launches over all pressure boxes and over all (axis, slab box) pairs
+    BoxLaunch pml_p_all{}, pml_aux_all{};
+    // z-slab of a larger grid (slab_nz > 0): local plane z is global plane
+    // z + slab_z0 of slab_nz planes; planes 0 and nz-1 are halos filled by
+    // the caller between step phases
+    int32_t slab_z0 = 0, slab_nz = 0;
+    int step_phase = 0;       // 0: whole steps; 1, 2: the halves of a split step
+    bool phase_open = false;  // the first half of a split step has run
+    int pml_p_blocks = 0, pml_aux_blocks = 0;
+    int pml_zc = 2;  // planes each PML thread marches
     int64_t pml_units = 0;
     int64_t n_pml_cells = 0;
     DBuf<int32_t> src_cell, src_begin;
@@ -1713,6 +1782,34 @@ void Engine::Impl::build_fused() {
     fused_dirty = false;
 }
 
+// The flat launch over `entries` (box, axis): blocks of 256 threads, w =
+// min(units, 32) units across, zc planes per thread; *blocks receives the
+// grid size.
+static BoxLaunch make_box_launch(const std::vector<std::pair<PmlBox, int>>& entries, int batch, int zc,
+                                 int* blocks) {
+    if ((int)entries.size() > kMaxLaunchBoxes) throw Error(AFD_ERR_ARG, "too many PML boxes for one launch");
+    BoxLaunch L{};
+    L.n = (int32_t)entries.size();
+    L.zc = zc;
+    int64_t start = 0;
+    for (size_t k = 0; k < entries.size(); ++k) {
+        const PmlBox& bx = entries[k].first;
+        const int w = std::min(bx.units, 32), rows = 256 / w;
+        L.box[k] = bx;
+        L.axis[k] = entries[k].second;
+        L.w[k] = w;
+        L.gx[k] = (bx.units + w - 1) / w;
+        L.gy[k] = (bx.height + rows - 1) / rows;
+        L.gzc[k] = (bx.depth + zc - 1) / zc;
+        L.start[k] = (int32_t)start;
+        start += (int64_t)L.gx[k] * L.gy[k] * L.gzc[k] * batch;
+    }
+    if (start >= ((int64_t)1 << 31)) throw Error(AFD_ERR_ARG, "PML launch too large");
+    L.start[entries.size()] = (int32_t)start;
+    *blocks = (int)start;
+    return L;
+}
+
 // SetPml (simulation.hpp:233-277) applied on the device: fresh auxiliary
 // fields, ksi profiles and, in FIXED mode, the PML cell list.
 void Engine::Impl::setup_pml() {
@@ -1727,6 +1824,9 @@ void Engine::Impl::setup_pml() {
     psi[1].release();
     pml_boxes.clear();
     for (auto& v : pml_axis_boxes) v.clear();
+    pml_p_all = BoxLaunch{};
+    pml_aux_all = BoxLaunch{};
+    pml_p_blocks = pml_aux_blocks = 0;
     pml_units = 0;
     n_pml_cells = 0;
     fused_dirty = true;
@@ -1754,7 +1854,9 @@ void Engine::Impl::setup_pml() {
         const uint32_t F = pml_faces;
         const int wpr = (int)(pitch / 32);
         pml_owned.alloc((size_t)nz * ny * wpr, false);
-        n_pml_cells = pml_masks_device(solid_view(), lrs_bits.ptr, nx, ny, nz, wpr, W, F, pml_owned.ptr, stream);
+        const int zoff = slab_nz > 0 ? slab_z0 : 0, nzg = slab_nz > 0 ? slab_nz : nz;
+        n_pml_cells = pml_masks_device(solid_view(), lrs_bits.ptr, nx, ny, nz, wpr, W, F, pml_owned.ptr, stream,
+                                       zoff, nzg);
         // disjoint boxes: z slabs take whole planes, y slabs the remaining
         // planes, x slabs the remaining rows
         pml_boxes.clear();
@@ -1769,13 +1871,17 @@ void Engine::Impl::setup_pml() {
             bx.depth = z1 - z0 + 1;
             pml_boxes.push_back(bx);
         };
-        int lo[3] = {2, 2, 2}, hi[3] = {nx - 3, ny - 3, nz - 3};
-        const int dims3[3] = {nx, ny, nz};
-        int rest_lo[3] = {2, 2, 2}, rest_hi[3] = {nx - 3, ny - 3, nz - 3};
+        // local coordinates; along z the grid may be a slab of a larger one
+        // (global plane = local + zoff), and the PML rules are global: cells
+        // 2..n-3 of the global grid, slabs of W planes at its global faces
+        const int off[3] = {0, 0, zoff};
+        const int dims3[3] = {nx, ny, nzg};
+        int lo[3] = {2, 2, std::max(2 - zoff, 1)}, hi[3] = {nx - 3, ny - 3, std::min(nzg - 3 - zoff, nz - 2)};
+        int rest_lo[3] = {lo[0], lo[1], lo[2]}, rest_hi[3] = {hi[0], hi[1], hi[2]};
         for (int ax = 2; ax >= 0; --ax) {
             const bool m_face = F & (1u << (2 * ax)), p_face = F & (2u << (2 * ax));
-            int mlo = lo[ax], mhi = std::min(W - 1, hi[ax]);
-            int plo = std::max(dims3[ax] - W, lo[ax]), phi = hi[ax];
+            int mlo = lo[ax], mhi = std::min(W - 1 - off[ax], hi[ax]);
+            int plo = std::max(dims3[ax] - W - off[ax], lo[ax]), phi = hi[ax];
             if (m_face && p_face && plo <= mhi) plo = mhi + 1;
             int box_lo[3], box_hi[3];
             for (int k = 0; k < 3; ++k) {
@@ -1806,8 +1912,8 @@ void Engine::Impl::setup_pml() {
         for (int ax = 0; ax < 3; ++ax) {
             pml_axis_boxes[ax].clear();
             const bool m_face = F & (1u << (2 * ax)), p_face = F & (2u << (2 * ax));
-            const int mhi = std::min(W - 1, hi[ax]);
-            int plo = std::max(dims3[ax] - W, lo[ax]);
+            const int mhi = std::min(W - 1 - off[ax], hi[ax]);
+            int plo = std::max(dims3[ax] - W - off[ax], lo[ax]);
             if (m_face && p_face && plo <= mhi) plo = mhi + 1;
             auto push = [&](int alo, int ahi) {
                 int l3[3] = {lo[0], lo[1], lo[2]}, h3[3] = {hi[0], hi[1], hi[2]};
@@ -1827,6 +1933,12 @@ void Engine::Impl::setup_pml() {
             if (p_face) push(plo, hi[ax]);
         }
         if ((int)pml_boxes.size() > kMaxPmlBoxes) throw Error(AFD_ERR_ARG, "too many PML boxes");
+        std::vector<std::pair<PmlBox, int>> pe, ae;
+        for (const PmlBox& bx : pml_boxes) pe.emplace_back(bx, 0);
+        for (int ax = 0; ax < 3; ++ax)
+            for (const PmlBox& bx : pml_axis_boxes[ax]) ae.emplace_back(bx, ax);
+        pml_p_all = make_box_launch(pe, prm.batch, pml_zc, &pml_p_blocks);
+        pml_aux_all = make_box_launch(ae, prm.batch, pml_zc, &pml_aux_blocks);
     }
 }
 
@@ -1962,6 +2074,8 @@ void Engine::Impl::build_args() {
     P.n_units = pml_units;
     P.cells = pml_owned.ptr;
     P.words_per_row = (int32_t)(pitch / 32);
+    P.zoff = slab_nz > 0 ? slab_z0 : 0;
+    P.nz_glob = slab_nz > 0 ? slab_nz : nz;
     a.src.n = (int32_t)src_cell.n;
     a.src.cell = src_cell.ptr;
     a.src.begin = src_begin.ptr;
@@ -2033,8 +2147,12 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         launch_stream<T>(plan.shape, fused_grid, st, tm_halo, tm_own, a, fdev, j);
         ++launches;
     };
-    const bool beside = lists_beside() && fdev.owned;
-    if (!beside) {
+    // a split step (z-slab runs): phase 1 runs the interior, boundary and
+    // PML pressure updates, phase 2 the PML auxiliary fields and the
+    // source/receiver and capture kernels, in the serial order
+    const bool phA = step_phase != 2, phB = step_phase != 1;
+    const bool beside = lists_beside() && fdev.owned && step_phase == 0;
+    if (!beside && phA) {
         if (use_fused()) {
             begin(KK_FUSED);
             stream_launch(stream);
@@ -2058,34 +2176,16 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         }
         ++launches;
     };
-    auto shape = [&](const PmlBox& bx, dim3& grd, dim3& bk) {
-        // rows of a narrow box packed side by side in a warp (no idle lanes)
-        const unsigned w = (unsigned)std::min(bx.units, 32);
-        bk = dim3(w, 256 / w, 1);
-        grd = dim3((unsigned)((bx.units + w - 1) / w), (unsigned)((bx.height + bk.y - 1) / bk.y),
-                   (unsigned)(bx.depth * prm.batch));
-    };
     const bool psi = a.pml.psi_on != 0;
-    auto pml_p_launch = [&](const PmlBox& bx, cudaStream_t st) {
-        dim3 grd, bk;
-        shape(bx, grd, bk);
-        if (psi) k_pml_box_p<true, T><<<grd, bk, 0, st>>>(a, bx, j);
-        else k_pml_box_p<false, T><<<grd, bk, 0, st>>>(a, bx, j);
+    // every pressure box in one launch, every (axis, slab box) pair in another
+    auto pml_p_launch = [&](cudaStream_t st) {
+        if (psi) k_pml_p_all<true, T><<<pml_p_blocks, 256, 0, st>>>(a, pml_p_all, j);
+        else k_pml_p_all<false, T><<<pml_p_blocks, 256, 0, st>>>(a, pml_p_all, j);
         ++launches;
     };
-    auto pml_aux_launch = [&](int ax, const PmlBox& bx, cudaStream_t st) {
-        dim3 grd, bk;
-        shape(bx, grd, bk);
-        if (ax == 0) {
-            if (psi) k_pml_box_aux<0, true, T><<<grd, bk, 0, st>>>(a, bx, j);
-            else k_pml_box_aux<0, false, T><<<grd, bk, 0, st>>>(a, bx, j);
-        } else if (ax == 1) {
-            if (psi) k_pml_box_aux<1, true, T><<<grd, bk, 0, st>>>(a, bx, j);
-            else k_pml_box_aux<1, false, T><<<grd, bk, 0, st>>>(a, bx, j);
-        } else {
-            if (psi) k_pml_box_aux<2, true, T><<<grd, bk, 0, st>>>(a, bx, j);
-            else k_pml_box_aux<2, false, T><<<grd, bk, 0, st>>>(a, bx, j);
-        }
+    auto pml_aux_launch = [&](cudaStream_t st) {
+        if (psi) k_pml_aux_all<true, T><<<pml_aux_blocks, 256, 0, st>>>(a, pml_aux_all, j);
+        else k_pml_aux_all<false, T><<<pml_aux_blocks, 256, 0, st>>>(a, pml_aux_all, j);
         ++launches;
     };
     bool src_done = false;  // the source/receiver kernel already queued beside the auxiliary updates
@@ -2103,35 +2203,29 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         std::vector<std::function<void(cudaStream_t)>> g1, g2;
         g1.push_back(stream_launch);
         if (a.lrs.n > 0) g1.push_back(lrs_launch);
-        if (fixed_pml)
-            for (const PmlBox& bx : pml_boxes) g1.push_back([&, bx](cudaStream_t st) { pml_p_launch(bx, st); });
-        if (fixed_pml)
-            for (int ax = 0; ax < 3; ++ax)
-                for (const PmlBox& bx : pml_axis_boxes[ax])
-                    g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
+        if (fixed_pml) g1.push_back(pml_p_launch);
+        if (fixed_pml) g2.push_back(pml_aux_launch);
         run_side_by_side(g1);
         run_side_by_side(g2);
-    } else if (fixed_pml && !profile && prm.graphs) {  // inside CUDA graphs: no host cost per step
+    } else if (fixed_pml && !profile && prm.graphs && step_phase == 0) {  // inside CUDA graphs: no host cost per step
         // FIXED scheme: the boundary update and the PML pressure boxes write
         // disjoint cells and read only levels n and n-1 and the old
         // auxiliary fields, so they run side by side; the auxiliary updates
         // (one per axis, disjoint outputs) follow once both are done.
         std::vector<std::function<void(cudaStream_t)>> g1, g2;
         if (a.lrs.n > 0) g1.push_back(lrs_launch);
-        for (const PmlBox& bx : pml_boxes) g1.push_back([&, bx](cudaStream_t st) { pml_p_launch(bx, st); });
+        g1.push_back(pml_p_launch);
         if (src_beside_aux && (a.src.n > 0 || a.rcv.n > 0)) {
             // queued first: its one block then starts at once instead of
             // waiting for the auxiliary updates' blocks to be dispatched
             g2.push_back([&](cudaStream_t st) { src_rcv_launch(st); });
             src_done = true;
         }
-        for (int ax = 0; ax < 3; ++ax)
-            for (const PmlBox& bx : pml_axis_boxes[ax])
-                g2.push_back([&, ax, bx](cudaStream_t st) { pml_aux_launch(ax, bx, st); });
+        g2.push_back(pml_aux_launch);
         run_side_by_side(g1);
         run_side_by_side(g2);
     } else {
-        if (a.lrs.n > 0) {
+        if (a.lrs.n > 0 && phA) {
             begin(KK_LRS);
             lrs_launch(stream);
             end();
@@ -2150,26 +2244,25 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
                     launches += 2;
                 }
             } else if (a.pml.n_units > 0) {
-                for (const PmlBox& bx : pml_boxes) {
+                if (phA) {
                     begin(KK_PML_P);
-                    pml_p_launch(bx, stream);
+                    pml_p_launch(stream);
                     end();
                 }
-                for (int ax = 0; ax < 3; ++ax)
-                    for (const PmlBox& bx : pml_axis_boxes[ax]) {
-                        begin(KK_PML_AUX);
-                        pml_aux_launch(ax, bx, stream);
-                        end();
-                    }
+                if (phB) {
+                    begin(KK_PML_AUX);
+                    pml_aux_launch(stream);
+                    end();
+                }
             }
         }
     }
-    if ((a.src.n > 0 || a.rcv.n > 0) && !src_done) {
+    if ((a.src.n > 0 || a.rcv.n > 0) && !src_done && phB) {
         begin(KK_SRC_RCV);
         src_rcv_launch(stream);
         end();
     }
-    if (cap_every > 0) {
+    if (cap_every > 0 && phB) {
         const int total = cap.rows * cap.cols;
         k_capture<T><<<(unsigned)std::min(592, (total + 255) / 256), 256, 0, stream>>>(a, cap, j);
         ++launches;
@@ -2231,8 +2324,7 @@ int64_t Engine::Impl::kernels_per_step() const {
     if (a.pml.width > 0) {
         if (ref()) k += (nx > 4 && ny > 4 && nz > 4) ? 2 : 0;
         else if (a.pml.n_units > 0)
-            k += (int64_t)pml_boxes.size() + (int64_t)pml_axis_boxes[0].size() + (int64_t)pml_axis_boxes[1].size() +
-                 (int64_t)pml_axis_boxes[2].size();
+            k += 2;
     }
     if (a.src.n > 0 || a.rcv.n > 0) ++k;
     if (cap_every > 0) ++k;
@@ -2300,6 +2392,93 @@ void Engine::set_stream(void* stream) {
         D.drop_graphs();
         D.stream = s;
     }
+}
+
+void Engine::set_slab(int32_t z_offset, int32_t nz_global) {
+    Impl& D = *d_;
+    if (D.phase_open) throw Error(AFD_ERR_STATE, "a split step is open");
+    if (nz_global == 0) {
+        D.slab_z0 = D.slab_nz = 0;
+    } else {
+        if (D.ref()) throw Error(AFD_ERR_STATE, "z-slabs need the FIXED scheme");
+        if (D.f16()) throw Error(AFD_ERR_STATE, "z-slabs need FP32 storage (FP16 scales are per grid)");
+        if (z_offset < 0 || nz_global < 3) throw Error(AFD_ERR_ARG, "bad slab placement");
+        D.slab_z0 = z_offset;
+        D.slab_nz = nz_global;
+    }
+    D.pml_dirty = true;  // the PML cells and boxes follow global planes
+}
+
+// Half of one time step (z-slab runs): phase 1 runs the interior, boundary
+// and PML pressure updates of step steps_done; phase 2 the PML auxiliary
+// updates, sources, receivers and capture, and completes the step. Between
+// them and after phase 2 the caller refreshes the halo planes (afd_halo).
+void Engine::step(int32_t phase) {
+    Impl& D = *d_;
+    if (phase != 1 && phase != 2) throw Error(AFD_ERR_ARG, "phase must be 1 or 2");
+    if ((phase == 1) == D.phase_open) throw Error(AFD_ERR_STATE, phase == 1 ? "phase 2 of the previous step is due"
+                                                                            : "phase 1 of this step has not run");
+    if (D.ref()) throw Error(AFD_ERR_STATE, "split steps need the FIXED scheme");
+    if (phase == 1) {
+        D.setup_run(1);
+        if (D.use_fused()) CK(cudaMemsetAsync(D.f_work.ptr, 0, sizeof(int), D.stream));
+        CK(cudaMemsetAsync(D.d_flag.ptr, 0, sizeof(int), D.stream));
+    }
+    D.step_phase = phase;
+    try {
+        D.launch_step(0, false);
+    } catch (...) {
+        D.step_phase = 0;
+        throw;
+    }
+    D.step_phase = 0;
+    if (phase == 2) {
+        k_advance<<<1, 1, 0, D.stream>>>(D.d_step.ptr, 1);
+        ++D.launches;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(D.stream));
+    int flag = 0;
+    CK(cudaMemcpy(&flag, D.d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    D.phase_open = phase == 1;
+    if (phase == 2) D.advance_done(1);
+    if (flag & 2) throw Error(AFD_ERR_CUDA, "step kernel pipeline wait timed out");
+    if (flag && D.prm.watchdog)
+        throw Error(AFD_ERR_NUMERIC, "pressure left the finite bound |p| < 1e30 by step " + std::to_string(D.steps_done));
+}
+
+// One plane of every batch member between the engine and a caller device
+// buffer ([batch][ny][pitch] floats): side 0 the low-z end, 1 the high-z
+// end; dir 0 reads the outermost interior plane of that end (local 1 or
+// nz-2), dir 1 writes the halo plane (local 0 or nz-1). field 0: the
+// pressure level of the open or last completed step; 1..3: that step's new
+// PML auxiliary field of axis x, y, z; 4: its new psi.
+void Engine::halo(int32_t side, int32_t dir, int32_t field, void* dev, int64_t cap) {
+    Impl& D = *d_;
+    if (!D.initialized || D.steps_done + (D.phase_open ? 1 : 0) == 0) throw Error(AFD_ERR_STATE, "no step has run");
+    if (side < 0 || side > 1 || dir < 0 || dir > 1 || field < 0 || field > 4) throw Error(AFD_ERR_ARG, "bad halo selector");
+    if (D.f16()) throw Error(AFD_ERR_STATE, "halo planes are FP32 levels");
+    const int64_t need = (int64_t)D.prm.batch * D.plane;
+    if (!dev || cap < need) throw Error(AFD_ERR_ARG, "halo buffer too small (batch * ny * pitch floats)");
+    const long long g = D.phase_open ? D.steps_done : D.steps_done - 1;
+    float* base = nullptr;
+    if (field == 0) {
+        base = D.fields.ptr + (size_t)buf_new(g) * D.vol * D.prm.batch;
+    } else {
+        if (D.pml_width <= 0 || !D.psi[0].ptr) throw Error(AFD_ERR_STATE, "no PML fields");
+        const int lv = (int)((g - D.pml_g0 + 1) & 1);
+        base = field == 4 ? D.psi[lv].ptr : D.fi[field - 1][lv].ptr;
+    }
+    const int64_t z = dir == 0 ? (side == 0 ? 1 : D.nz - 2) : (side == 0 ? 0 : D.nz - 1);
+    CK(cudaSetDevice(D.device));
+    float* d = static_cast<float*>(dev);
+    for (int32_t b = 0; b < D.prm.batch; ++b) {
+        float* lvl = base + (size_t)b * D.vol + (size_t)z * D.plane;
+        float* buf = d + (size_t)b * D.plane;
+        if (dir == 0) CK(cudaMemcpyAsync(buf, lvl, (size_t)D.plane * sizeof(float), cudaMemcpyDeviceToDevice, D.stream));
+        else CK(cudaMemcpyAsync(lvl, buf, (size_t)D.plane * sizeof(float), cudaMemcpyDeviceToDevice, D.stream));
+    }
+    CK(cudaStreamSynchronize(D.stream));
 }
 
 void Engine::set_plan(const afd_plan* p) {

@@ -48,6 +48,9 @@ public:
     double energy(int32_t batch);
     void set_stream(void* stream);
     void set_plan(const afd_plan* plan);
+    void set_slab(int32_t z_offset, int32_t nz_global);
+    void step(int32_t phase);
+    void halo(int32_t side, int32_t dir, int32_t field, void* dev, int64_t cap);
     float cell_size() const;
     int kernel_stats(int32_t idx, char* name, int64_t cap, int64_t* launches, double* ms);
 

@@ -238,17 +238,20 @@ __global__ void k_cell_bits(const int32_t* __restrict__ cells, int64_t n, uint32
 }
 
 // one thread per word of the engine grid
+// zoff, gzg: the grid's planes are global planes zoff.. of a grid of gzg
+// planes (a z-slab of it); the slab rules use global planes.
 __global__ void k_pml_masks(SolidBits s, const uint32_t* __restrict__ lrs, int gx, int gy, int gz, int wpr, int W,
-                            uint32_t F, uint32_t* owned, unsigned long long* count) {
+                            uint32_t F, uint32_t* owned, unsigned long long* count, int zoff, int gzg) {
     const int64_t total = (int64_t)gz * gy * wpr;
     unsigned long long n = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t w = i % wpr, y = i / wpr % gy, z = i / wpr / gy;
+        const int64_t zg = z + zoff;
         const uint32_t a = ~solid_word(s, w, y, z) & ~lrs[i] & range_bits(w, 0, gx - 1);
         uint32_t o = 0u;
-        if (a && y >= 2 && y <= gy - 3 && z >= 2 && z <= gz - 3) {
+        if (a && y >= 2 && y <= gy - 3 && zg >= 2 && zg <= gzg - 3 && z >= 1 && z <= gz - 2) {
             const bool yz = ((F & AFD_FACE_YM) && y < W) || ((F & AFD_FACE_YP) && y > gy - W - 1) ||
-                            ((F & AFD_FACE_ZM) && z < W) || ((F & AFD_FACE_ZP) && z > gz - W - 1);
+                            ((F & AFD_FACE_ZM) && zg < W) || ((F & AFD_FACE_ZP) && zg > gzg - W - 1);
             uint32_t slab = yz ? 0xffffffffu : 0u;
             if (F & AFD_FACE_XM) slab |= range_bits(w, 0, W - 1);
             if (F & AFD_FACE_XP) slab |= range_bits(w, gx - W, gx - 1);
@@ -376,13 +379,15 @@ void boundary_bits_device(const int32_t* d_cells, int64_t n, int64_t words, uint
 }
 
 int64_t pml_masks_device(const SolidBits& s, const uint32_t* d_boundary, int32_t gx, int32_t gy, int32_t gz,
-                         int32_t wpr, int32_t width, uint32_t faces, uint32_t* d_owned, void* stream) {
+                         int32_t wpr, int32_t width, uint32_t faces, uint32_t* d_owned, void* stream, int32_t zoff,
+                         int32_t gz_global) {
     cudaStream_t st = (cudaStream_t)stream;
     if ((int64_t)wpr * 32 < gx) throw Error(AFD_ERR_ARG, "mask rows narrower than the grid");
     Scratch<unsigned long long> cnt(1);
     GK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned long long), st));
     const int64_t words = (int64_t)gz * gy * wpr;
-    k_pml_masks<<<grid_for(words, 256), 256, 0, st>>>(s, d_boundary, gx, gy, gz, wpr, width, faces, d_owned, cnt.p);
+    k_pml_masks<<<grid_for(words, 256), 256, 0, st>>>(s, d_boundary, gx, gy, gz, wpr, width, faces, d_owned, cnt.p,
+                                                       zoff, gz_global > 0 ? gz_global : gz);
     GK(cudaGetLastError());
     unsigned long long h = 0;
     GK(cudaMemcpyAsync(&h, cnt.p, sizeof h, cudaMemcpyDeviceToHost, st));

@@ -53,14 +53,17 @@ void solid_bits_device(const int32_t* d_vox, int32_t nx, int32_t ny, int32_t nz,
 //                         neither solid nor boundary, with 2 <= x,y,z <= n-3,
 //                         inside an enabled face slab of `width` cells, into
 //                         d_owned; returns their number (synchronises
-//                         `stream`)
+//                         `stream`). zoff, gz_global: the grid is a z-slab
+//                         (planes zoff.. of gz_global); the rules then use
+//                         global planes and skip the slab's two end planes
 //   or_masks_device       out = a | b over n words (a may be null)
 //   air_flags_device      flags[z][ty * tiles_x + tx] = 1 where an air cell
 //                         lies in tile (tx, ty) of plane z widened by one
 //                         cell in x and y (tiles tile_w x tile_h)
 void boundary_bits_device(const int32_t* d_cells, int64_t n, int64_t words, uint32_t* d_bits, void* stream);
 int64_t pml_masks_device(const SolidBits& s, const uint32_t* d_boundary, int32_t gx, int32_t gy, int32_t gz,
-                         int32_t wpr, int32_t width, uint32_t faces, uint32_t* d_owned, void* stream);
+                         int32_t wpr, int32_t width, uint32_t faces, uint32_t* d_owned, void* stream,
+                         int32_t zoff = 0, int32_t gz_global = 0);
 void or_masks_device(const uint32_t* a, const uint32_t* b, uint32_t* out, int64_t n, void* stream);
 void air_flags_device(const SolidBits& s, int32_t gx, int32_t gy, int32_t gz, int32_t tile_w, int32_t tile_h,
                       int32_t tiles_x, int32_t tiles_y, uint8_t* d_flags, void* stream);

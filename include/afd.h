@@ -331,6 +331,35 @@ typedef struct afd_plan {
  * results bit for bit. */
 int afd_set_plan(afd_sim* s, const afd_plan* plan);
 
+/* z-slab domain decomposition (no counterpart in the reference, which runs
+ * one device: simulation.hpp:176-178, 356-402). The simulation's grid is
+ * global planes z_offset .. z_offset+nz-1 of a grid of nz_global planes:
+ * its planes 0 and nz-1 are halos (or the global end faces) that the caller
+ * fills from the neighbouring slabs, its planes 1..nz-2 are its own; the
+ * PML cell rule and the z slabs of the PML use global planes. FIXED scheme
+ * and FP32 storage only. nz_global = 0 turns it off. */
+int afd_set_slab(afd_sim* s, int32_t z_offset, int32_t nz_global);
+
+/* One half of the next time step, launched in the serial order (no graphs):
+ * phase 1 the interior, boundary and PML pressure updates; phase 2 the PML
+ * auxiliary updates, sources, receivers and capture, which completes the
+ * step. A slab run refreshes the high-z halo of the new pressure (and psi)
+ * between the phases, where the auxiliary update of its last plane reads
+ * it, and both halos of the new pressure and the new auxiliary fields after
+ * phase 2. Call afd_prepare(total steps) first to size the receiver record.
+ * Synchronous. */
+int afd_step_phase(afd_sim* s, int32_t phase);
+
+/* Copies one plane of every batch member between the simulation and the
+ * caller's device buffer dev ([batch][ny][pitch] floats, pitch = nx rounded
+ * up to 32; cap in floats). side 0: the low-z end, 1: the high-z end. dir 0
+ * reads the outermost own plane of that end (local 1 or nz-2) into dev,
+ * dir 1 writes dev into the halo plane (local 0 or nz-1). field 0: the
+ * pressure level of the open (after phase 1) or last completed step;
+ * 1, 2, 3: that step's new PML auxiliary field of axis x, y, z; 4: its new
+ * psi. Synchronous. */
+int afd_halo(afd_sim* s, int32_t side, int32_t dir, int32_t field, void* dev, int64_t cap);
+
 /* Per-kernel statistics of the last afd_run made with params.profile set:
  * kernel idx (0-based) -> name, launches and summed device milliseconds.
  * Returns AFD_ERR_ARG when idx is past the last kernel. */
