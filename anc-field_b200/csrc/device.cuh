@@ -198,17 +198,26 @@ struct StepScales {
     float s_old, inv_old;  // level g - 2 (p^{n-1})
 };
 
-// The slots read here (levels g-2..g-4) are written only by the interior
-// kernels of earlier steps (step g writes slot g-1 and clears slot g), so
-// they are read through the read-only cache: one L2 request per SM instead
-// of one per warp at the same address. 1/s is 2^-k exactly (what 1.0f / s
-// gives for a power of two).
+// Slot load through L2 only (ld.global.cg): the slots are written inside
+// the same CUDA graph by the interior kernels of earlier steps (step g
+// writes slot g-1 and clears slot g) while other kernels of a step may read
+// the neighbouring slots of the same sector, so they are never read through
+// the SM's non-coherent read-only cache, which could keep a sector fetched
+// before its slots were final.
+__device__ __forceinline__ uint32_t ld_slot(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+// Scales of levels g, g-1, g-2 from the slots of levels g-2..g-4. 1/s is
+// 2^-k exactly (what 1.0f / s gives for a power of two).
 __device__ __forceinline__ StepScales step_scales(const F16Dev& f, int b, long long g) {
     const uint32_t* mx = f.mx + (size_t)b * 5;
     const float smax = __ldg(f.src_max + b);
-    const int kn = level_scale_exp(__ldg(mx + max_slot(g - 2)), smax);
-    const int kc = level_scale_exp(__ldg(mx + max_slot(g - 3)), smax);
-    const int ko = level_scale_exp(__ldg(mx + max_slot(g - 4)), smax);
+    const int kn = level_scale_exp(ld_slot(mx + max_slot(g - 2)), smax);
+    const int kc = level_scale_exp(ld_slot(mx + max_slot(g - 3)), smax);
+    const int ko = level_scale_exp(ld_slot(mx + max_slot(g - 4)), smax);
     StepScales s;
     s.s_new = pow2_exact(kn);
     s.s_cur = pow2_exact(kc);

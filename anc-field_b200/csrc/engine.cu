@@ -1055,7 +1055,7 @@ __device__ __forceinline__ float2 new_level_scale(const StepArgs& a, int b, long
     if constexpr (sizeof(T) == 4) {
         return make_float2(1.0f, 1.0f);
     } else {
-        const int k = level_scale_exp(__ldg(a.f16.mx + (size_t)b * 5 + max_slot(g - 2)), __ldg(a.f16.src_max + b));
+        const int k = level_scale_exp(ld_slot(a.f16.mx + (size_t)b * 5 + max_slot(g - 2)), __ldg(a.f16.src_max + b));
         return make_float2(pow2_exact(k), pow2_exact(-k));
     }
 }

@@ -98,6 +98,79 @@ __global__ void k_passive(const double* a, const double* b, int nmat, int K, int
     }
 }
 
+// The same two checks for at most MAXC coefficients without local memory
+// (no per-thread stack to reserve at launch): the Durand-Kerner iterates of
+// the root kernel live in shared memory, one row per thread, and the
+// passivity kernel evaluates e^{-jwk} with sincospi (w = pi f / (nf - 1), so
+// the argument is the exact fraction -k f / (nf - 1) and needs no reduction
+// table). Same iteration as max_root_of; the frequency grid of k_passive.
+template <int MAXC>
+__global__ void __launch_bounds__(64) k_roots_static(const double* b, int nmat, int K, double* out) {
+    __shared__ C zs[64][MAXC];
+    __shared__ double ms[64][MAXC];
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmat) return;
+    C* z = zs[threadIdx.x];
+    double* mono = ms[threadIdx.x];
+    const double* c = b + (size_t)m * K;
+    const int n = K - 1;
+    if (n <= 0) {
+        out[m] = 0.0;
+        return;
+    }
+    if (c[0] == 0.0) {
+        out[m] = INFINITY;
+        return;
+    }
+    for (int k = 0; k <= n; ++k) mono[k] = c[k] / c[0];
+    C seed{0.4, 0.9}, p{1.0, 0.0};
+    for (int k = 0; k < n; ++k) {
+        z[k] = p;
+        p = cmul(p, seed);
+    }
+    for (int it = 0; it < 2000; ++it) {
+        double moved = 0.0;
+        for (int k = 0; k < n; ++k) {
+            C v{1.0, 0.0};
+            for (int q = 1; q <= n; ++q) v = cadd(cmul(v, z[k]), C{mono[q], 0.0});
+            C den{1.0, 0.0};
+            for (int q = 0; q < n; ++q)
+                if (q != k) den = cmul(den, csub(z[k], z[q]));
+            const C step = cdiv(v, den);
+            z[k] = csub(z[k], step);
+            moved = fmax(moved, cabs_(step));
+        }
+        if (moved < 1e-15) break;
+    }
+    double mr = 0.0;
+    for (int k = 0; k < n; ++k) mr = fmax(mr, cabs_(z[k]));
+    out[m] = mr;
+}
+
+__global__ void k_passive_static(const double* a, const double* b, int nmat, int K, int nf, double* out) {
+    const int m = blockIdx.y;
+    double lo = INFINITY;
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nf; f += gridDim.x * blockDim.x) {
+        C A{0.0, 0.0}, B{0.0, 0.0};
+        for (int k = 0; k < K; ++k) {
+            double sn, cs;
+            sincospi(-(double)(k * f) / (double)(nf - 1), &sn, &cs);
+            A = cadd(A, C{a[(size_t)m * K + k] * cs, a[(size_t)m * K + k] * sn});
+            B = cadd(B, C{b[(size_t)m * K + k] * cs, b[(size_t)m * K + k] * sn});
+        }
+        lo = fmin(lo, cdiv(A, B).re);
+    }
+    for (int o = 16; o > 0; o >>= 1) lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    __shared__ double part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = lo;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = part[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) v = fmin(v, part[k]);
+        out[(size_t)m * gridDim.x + blockIdx.x] = v;
+    }
+}
+
 #define CKF(call)                                                                        \
     do {                                                                                 \
         cudaError_t e__ = (call);                                                        \
@@ -219,8 +292,8 @@ void check_filters_static(int32_t nmat, int32_t K, const double* a, const double
     // slots are cleared anyway so that a failed launch cannot hand back the
     // previous call's values
     CKF(cudaMemset(dr, 0, (size_t)(kStaticMaxMat + kStaticMaxMat * kStaticBlocks) * sizeof(double)));
-    k_roots<<<(nmat + 63) / 64, 64>>>(db, nmat, K, dr);
-    k_passive<<<dim3(kStaticBlocks, nmat), 256>>>(da, db, nmat, K, nf, dl);
+    k_roots_static<kStaticMaxCoef><<<(nmat + 63) / 64, 64>>>(db, nmat, K, dr);
+    k_passive_static<<<dim3(kStaticBlocks, nmat), 256>>>(da, db, nmat, K, nf, dl);
     CKF(cudaGetLastError());
     double roots[kStaticMaxMat];
     double part[kStaticMaxMat * kStaticBlocks];

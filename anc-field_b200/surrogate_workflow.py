@@ -283,3 +283,203 @@ def geometric_inputs(x):
             img[:, ax] = 2 * wall - s[:, ax]
             d.append(np.linalg.norm(img - r, axis=1))
     return np.concatenate([x, (np.stack(d, axis=1) / diag).astype(np.float32)], axis=1).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Field readout: the IR at any receiver position of a (wall set, source)
+# whose batched FDTD run recorded a grid of receivers.
+# ---------------------------------------------------------------------------
+GRID_H = 0.15  # m, spacing of the recorded receiver grid (about 9 points per wavelength at 250 Hz)
+
+
+def receiver_grid(h=GRID_H):
+    """Receiver cells on a regular grid of spacing h metres inside the
+    MARGIN-cell band of the walls, in x-fastest order."""
+    nx, ny, nz = ROOM
+    step = max(1, int(round(h / DX)))
+    axes = [np.arange(MARGIN, n - MARGIN, step) for n in (nx, ny, nz)]
+    zz, yy, xx = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1).astype(np.int32)
+
+
+def _pad_rows(t, m):
+    import torch
+    r = (-t.shape[0]) % m
+    return t if r == 0 else torch.cat([t, t.new_zeros((r,) + tuple(t.shape[1:]))])
+
+
+def _pad_cols(t, m):
+    import torch
+    r = (-t.shape[1]) % m
+    return t if r == 0 else torch.cat([t, t.new_zeros((t.shape[0], r))], dim=1)
+
+
+def gemm_split(pkg, a, b):
+    """c = a @ b^T in FP32 from FP32 device matrices through the tcgen05 BF16
+    GEMM: each operand split into a BF16 value and a BF16 remainder, and the
+    three products that carry FP32-level accuracy summed (the remainder's
+    product with the remainder is below FP32 resolution). Rows are padded
+    to 128 and the shared dimension to 64 with zeros."""
+    import torch
+    M, N = a.shape[0], b.shape[0]
+    a = _pad_cols(_pad_rows(a, 128), 64)
+    b = _pad_cols(_pad_rows(b, 128), 64)
+    ah = a.to(torch.bfloat16)
+    al = (a - ah.float()).to(torch.bfloat16)
+    bh = b.to(torch.bfloat16)
+    bl = (b - bh.float()).to(torch.bfloat16)
+    c = torch.empty(a.shape[0], b.shape[0], dtype=torch.float32, device=a.device)
+    t = torch.empty_like(c)
+    st = torch.cuda.current_stream().cuda_stream
+    G = pkg.surrogate.gemm_bf16
+    G(ah, bh, c, st)
+    G(ah, bl, t, st)
+    c += t
+    G(al, bh, t, st)
+    c += t
+    return c[:M, :N]
+
+
+class FieldReadout:
+    """IR at a receiver position as a linear readout of D random Fourier
+    features of the position (metres): phi(r) = sqrt(2 / D) cos(W r + c),
+    W ~ N(0, sigma^2) rad/m, c ~ U(0, 2 pi) -- a one-hidden-layer network
+    whose hidden layer is fixed and whose output layer is fitted by ridge
+    regression through the normal equations: the Gram matrix Phi^T Phi and
+    Phi^T Y come from the tcgen05 GEMM (split BF16), the D x D system is
+    solved in FP64. One readout serves every (wall set, source) recorded at
+    the same receiver positions: their IRs are the columns of Y."""
+
+    def __init__(self, pkg, n_feat=4096, sigma=6.0, ridge=1e-6, seed=0):
+        import torch
+        self.pkg = pkg
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        self.W = (torch.randn(3, n_feat, generator=g, dtype=torch.float64) * sigma).float().cuda()
+        self.c = (torch.rand(n_feat, generator=g, dtype=torch.float64) * 2 * math.pi).float().cuda()
+        self.n_feat, self.ridge = n_feat, ridge
+        self.beta = None
+
+    def features(self, cells):
+        import torch
+        r = torch.as_tensor(np.asarray(cells, np.float64) * DX, dtype=torch.float32, device="cuda")
+        return math.sqrt(2.0 / self.n_feat) * torch.cos(r @ self.W + self.c)
+
+    def fit(self, cells, y):
+        """cells [N, 3]; y [N, L] (device or host, FP32): one column block per
+        (wall set, source)."""
+        import torch
+        phi = self.features(cells)                          # [N, D]
+        pt = phi.t().contiguous()                           # [D, N]
+        y = torch.as_tensor(y, dtype=torch.float32, device="cuda")
+        gram = gemm_split(self.pkg, pt, pt).double()        # [D, D]
+        rhs = gemm_split(self.pkg, pt, y.t().contiguous()).double()  # [D, L]
+        lam = self.ridge * torch.trace(gram) / self.n_feat
+        gram.diagonal().add_(lam)
+        L = torch.linalg.cholesky(gram)
+        self.beta = torch.cholesky_solve(rhs, L).float()    # [D, L]
+        self.beta_t = self.beta.t().contiguous()            # [L, D]
+        return self
+
+    def predict(self, cells):
+        """[Q, L] FP32 device tensor: the readout at receiver cells."""
+        return gemm_split(self.pkg, self.features(cells), self.beta_t)
+
+
+def field_irs(pkg, g, src_cells, rcv_cells):
+    """One batched FDTD run of wall set g: IRs [n_src, n_rcv, IR_LEN] on
+    the device, and the run's wall seconds (setup excluded)."""
+    import torch
+    irs, wall = batched_irs(pkg, g, src_cells, rcv_cells)
+    return torch.from_numpy(irs).cuda(), wall
+
+
+def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, seed=21, n_feat=4096,
+                      sigma=6.0, grid_h=GRID_H, plain=True):
+    """The learned readout against the FDTD for receiver positions that the
+    generating runs did not record as training data (new positions, the
+    runs' own wall sets and sources; the query and validation receivers are
+    recorded in the same runs as the FDTD answer). Per wall set: one batched
+    FDTD run of n_src sources with the receiver grid, n_query query and
+    n_val validation receivers. The readout is fitted on the grid; a
+    committee of two readouts fitted on the two halves of the grid gives
+    each pair a predicted error (their disagreement, calibrated on the
+    validation receivers), and a pair whose predicted error exceeds `bound`
+    falls back to the FDTD: one plain single-source run per (wall set,
+    source) that has such a pair. Without the readout every query pair
+    needs the FDTD: one batched run per wall set. Reports errors, the
+    fraction within the bound, IRs/s of each path and the gain."""
+    import torch
+    rng = np.random.default_rng(seed)
+    grid = receiver_grid(grid_h)
+    gsets = [rng.uniform(G_LO, G_HI, 4) for _ in range(n_sets)]
+    srcs = [random_cells(rng, n_src) for _ in range(n_sets)]
+    q_cells = random_cells(rng, n_query)
+    v_cells = random_cells(rng, n_val)
+    rcv = np.concatenate([grid, q_cells, v_cells])
+    ng = len(grid)
+    Y_grid, Y_q, Y_v, fd_s = [], [], [], []
+    for w in range(n_sets):
+        irs, wall = field_irs(pkg, gsets[w], srcs[w], rcv)
+        fd_s.append(wall)
+        Y_grid.append(irs[:, :ng])            # [S, G, L]
+        Y_q.append(irs[:, ng:ng + n_query])
+        Y_v.append(irs[:, ng + n_query:])
+        del irs
+    # columns: (wall set, source, sample)
+    yg = torch.cat([t.permute(1, 0, 2).reshape(ng, -1) for t in Y_grid], dim=1)
+    scale = float(yg.pow(2).mean().sqrt())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    full = FieldReadout(pkg, n_feat=n_feat, sigma=sigma, seed=seed).fit(grid, yg / scale)
+    half = [FieldReadout(pkg, n_feat=n_feat, sigma=sigma, seed=seed).fit(grid[k::2], yg[k::2] / scale)
+            for k in range(2)]
+    torch.cuda.synchronize()
+    t_fit = time.perf_counter() - t0
+
+    def split_pairs(pred, n):
+        # [n, n_sets * n_src * L] -> [n_sets, n_src, n, L]
+        return pred.reshape(n, n_sets, n_src, IR_LEN).permute(1, 2, 0, 3)
+
+    def rel(a, b):
+        return ((a - b).norm(dim=-1) / b.norm(dim=-1).clamp_min(1e-30)).cpu().numpy()
+
+    yv = torch.stack(Y_v) / scale
+    pv = split_pairs(full.predict(v_cells), n_val)
+    dv = rel(split_pairs(half[0].predict(v_cells), n_val), split_pairs(half[1].predict(v_cells), n_val))
+    ev = rel(pv, yv)
+    calib = float(np.median(ev / np.maximum(dv, 1e-12)))  # true error per unit of committee disagreement
+    yq = torch.stack(Y_q) / scale
+    full.predict(q_cells[:8])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pq = split_pairs(full.predict(q_cells), n_query)
+    dq = rel(split_pairs(half[0].predict(q_cells), n_query), split_pairs(half[1].predict(q_cells), n_query))
+    torch.cuda.synchronize()
+    t_pred = time.perf_counter() - t0
+    eq = rel(pq, yq)                           # [n_sets, n_src, n_query]
+    pe = calib * dq
+    accept = pe <= bound
+    runs_needed = int((~accept).any(axis=2).sum())
+    t_plain = None
+    if plain:
+        _, t_plain = plain_irs(pkg, gsets[0], srcs[0][0], q_cells[:16])
+    t_single = t_plain if t_plain is not None else float(np.mean(fd_s)) / n_src
+    n_pairs = n_sets * n_src * n_query
+    t_fallback = runs_needed * t_single
+    fdtd_alone_s = float(np.sum(fd_s))  # one batched run per wall set answers every query pair
+    irs_fdtd = n_pairs / fdtd_alone_s
+    irs_sur = n_pairs / (t_pred + t_fallback)
+    return {
+        "wall_sets": n_sets, "sources_per_set": n_src, "grid_receivers": ng, "grid_spacing_m": grid_h,
+        "query_pairs": n_pairs, "validation_pairs": n_sets * n_src * n_val, "features": n_feat,
+        "sigma_rad_per_m": sigma, "fit_s": t_fit, "fdtd_run_s": fd_s,
+        "query_rel_l2": {"median": float(np.median(eq)), "p90": float(np.percentile(eq, 90)),
+                         "max": float(eq.max())},
+        "validation_median_rel_l2": float(np.median(ev)),
+        "within_bound": float((eq <= bound).mean()), "accepted": float(accept.mean()),
+        "accepted_but_over_bound": int((accept & (eq > bound)).sum()),
+        "fallback_runs": runs_needed,
+        "irs_per_s": {"readout_only": n_pairs / t_pred, "readout_with_fallback": irs_sur,
+                      "batched_fdtd": irs_fdtd, "plain_fdtd": (16 / t_plain) if t_plain else None},
+        "gain_over_fdtd": irs_sur / irs_fdtd, "bound": bound,
+    }

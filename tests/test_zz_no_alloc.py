@@ -147,12 +147,13 @@ def test_static_runs_with_no_device_memory_left(pkg):
                 raw.append(p)
         rc0, _, _, _ = _call(lib, "afd_check_filters", a, b)
         rc1, st1, mr1, _ = _call(lib, "afd_check_filters_static", a, b)
+        msg = lib.afd_model_last_error(None)
     finally:
         for p in raw:
             rt.cudaFree(p)
         hold.clear()
         torch.cuda.empty_cache()
     assert rc0 == pkg.afd.ERR_CUDA
-    assert rc1 == 0
+    assert rc1 == 0, msg
     assert np.array_equal(st1, st_ref)
     np.testing.assert_allclose(mr1, mr_ref, rtol=RTOL, atol=0.0)
