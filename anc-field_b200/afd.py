@@ -67,12 +67,12 @@ class Info(C.Structure):
                 ("last_run_ms", C.c_double), ("kernel_launches", C.c_int64),
                 ("tile_x", C.c_int32), ("tile_y", C.c_int32), ("tile_z", C.c_int32),
                 ("stream_blocks", C.c_int32), ("tuned", C.c_int32), ("stream_beside", C.c_int32),
-                ("stream_per_sm", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("stream_per_sm", C.c_int32), ("stream_tail", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class Plan(C.Structure):
     _fields_ = [("tile_x", C.c_int32), ("tile_y", C.c_int32), ("per_sm", C.c_int32), ("dz", C.c_int32),
-                ("beside", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("beside", C.c_int32), ("tail", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_int64, C.c_void_p)
@@ -450,14 +450,15 @@ class Simulation:
     def set_stream(self, stream_handle):
         self._check(library().afd_set_stream(self._h, C.c_void_p(stream_handle)))
 
-    def set_plan(self, tile=(0, 0), per_sm=0, dz=0, beside=False, auto=False):
+    def set_plan(self, tile=(0, 0), per_sm=0, dz=0, beside=False, tail=False, auto=False):
         """Fixes the streaming kernel's plan (tile in cells, resident blocks
-        per SM, z-chunk depth, boundary/PML kernels beside it) and turns the
-        online autotuner off; auto=True gives the choice back to it."""
+        per SM, z-chunk depth, boundary/PML kernels beside it or in its tail
+        warps) and turns the online autotuner off; auto=True gives the
+        choice back to it."""
         if auto:
             self._check(library().afd_set_plan(self._h, None))
             return
-        p = Plan(tile[0], tile[1], per_sm, dz, 1 if beside else 0)
+        p = Plan(tile[0], tile[1], per_sm, dz, 1 if beside else 0, 1 if tail else 0)
         self._check(library().afd_set_plan(self._h, C.byref(p)))
 
     # --- z-slab decomposition ----------------------------------------

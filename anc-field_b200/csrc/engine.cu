@@ -124,13 +124,10 @@ __global__ void __launch_bounds__(256) k_interior(StepArgs a, int j) {
 // T: level storage (FP16 only with the FIXED scheme).
 // Memory-latency-bound gathers: 5 blocks per SM (48 registers, no spills
 // for the FIXED variants) keep more loads in flight than 4.
+// One boundary point e of batch member b at global step g: reads p^n and
+// p^{n-1} around the cell, writes p^{n+1} of the cell and its filter state.
 template <bool REF, int KT, typename T>
-__global__ void __launch_bounds__(256, 5) k_lrs(const __grid_constant__ StepArgs a, int j) {
-    const long long g = *a.d_step + j;
-    const TlMark tl(a, 1, g, blockIdx.y == 0);
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.lrs.n) return;
-    const int b = blockIdx.y;
+__device__ __forceinline__ void lrs_update(const StepArgs& a, int b, int e, long long g) {
     const size_t base = (size_t)b * a.g.vol;
     T* pn = level_ptr<T>(a, buf_new(g)) + base;
     const T* pc = level_ptr<T>(a, buf_cur(g)) + base;
@@ -160,6 +157,15 @@ __global__ void __launch_bounds__(256, 5) k_lrs(const __grid_constant__ StepArgs
     if constexpr (sizeof(T) == 2) {
         if (!f16_finite(v * s_new)) atomicOr(a.flag, 1);
     }
+}
+
+template <bool REF, int KT, typename T>
+__global__ void __launch_bounds__(256, 5) k_lrs(const __grid_constant__ StepArgs a, int j) {
+    const long long g = *a.d_step + j;
+    const TlMark tl(a, 1, g, blockIdx.y == 0);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.lrs.n) return;
+    lrs_update<REF, KT, T>(a, (int)blockIdx.y, e, g);
 }
 
 template <bool REF, typename T>
@@ -743,8 +749,57 @@ __device__ __forceinline__ void cvt8(const uint4 w, float v[8]) {
 // only its own rows. T = __half: FP16 levels, the update evaluated on the
 // stored values (slf_update_scaled) and the largest |p^n| of every work
 // item gathered for the scale of level g + 1.
-template <typename T, int S>
-__global__ void __launch_bounds__(F_THREADS, 2)
+// The tail warps of the streaming kernel (FP32 storage, FIXED scheme): the
+// step's boundary points and PML pressure units, taken 32 at a time from a
+// per-step counter, while the other warps stream the interior (which skips
+// those cells through the owned-cell mask). Both read only p^n, p^{n-1},
+// the filter state and the previous auxiliary fields, and write disjoint
+// cells; the order of the work items does not change any result.
+constexpr int kTailWarps = 4;
+
+__device__ __forceinline__ void stream_tail(const StepArgs& a, const FusedDev& f, int j, long long g) {
+    const int lane = threadIdx.x & 31;
+    const long long B = a.batch;
+    const long long n_lrs = (long long)a.lrs.n * B;
+    const bool pml = a.mode != AFD_MODE_REF && a.pml.width > 0 && a.pml.n_units > 0;
+    const long long total = n_lrs + (pml ? a.pml.n_units * B : 0);
+    const int K = a.lrs.K;
+    const bool psi = a.pml.psi_on != 0;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(f.tail + j, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((long long)base >= total) break;
+        const long long u = (long long)base + lane;
+        if (u < n_lrs) {
+            const int b = (int)(u / a.lrs.n), e = (int)(u - (long long)b * a.lrs.n);
+            switch (K) {
+                case 1: lrs_update<false, 1, float>(a, b, e, g); break;
+                case 2: lrs_update<false, 2, float>(a, b, e, g); break;
+                case 3: lrs_update<false, 3, float>(a, b, e, g); break;
+                case 4: lrs_update<false, 4, float>(a, b, e, g); break;
+                default: lrs_update<false, 0, float>(a, b, e, g); break;
+            }
+        } else if (u < total) {
+            const PmlDev& P = a.pml;
+            long long r = u - n_lrs;
+            const int b = (int)(r / P.n_units);
+            r -= (long long)b * P.n_units;
+            int k = 0;
+            while (k + 1 < P.n_boxes && r >= P.boxes[k + 1].first) ++k;
+            const PmlBox& bx = P.boxes[k];
+            r -= bx.first;
+            const int ux = (int)(r % bx.units);
+            r /= bx.units;
+            const int yy = (int)(r % bx.height), zz = (int)(r / bx.height);
+            if (psi) pml_p_unit<true, float>(a, b, bx.x0 + 4 * ux, bx.y0 + yy, bx.z0 + zz, g, 1.0f, 1.0f, 1.0f);
+            else pml_p_unit<false, float>(a, b, bx.x0 + 4 * ux, bx.y0 + yy, bx.z0 + zz, g, 1.0f, 1.0f, 1.0f);
+        }
+    }
+}
+
+template <typename T, int S, bool TAIL = false>
+__global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS, 2)
     k_stream(const __grid_constant__ CUtensorMap tm_halo, const __grid_constant__ CUtensorMap tm_own,
              const __grid_constant__ StepArgs a, const __grid_constant__ FusedDev f, int j) {
     const TlMark tl(a, 0, *a.d_step + j, true);
@@ -768,6 +823,12 @@ __global__ void __launch_bounds__(F_THREADS, 2)
     const int B = a.batch, nz = a.g.nz;
     const int n_items = f.items ? f.n_items : f.tiles_x * f.tiles_y * f.n_chunks * B;
     const int wn = buf_new(g), wc = buf_cur(g), wo = buf_old(g);
+    if constexpr (TAIL && sizeof(T) == 4) {
+        if (tid >= F_THREADS) {
+            stream_tail(a, f, j, g);
+            return;
+        }
+    }
 
     if (tid >= F_CONSUMERS) {
         // producer: takes work items from the launch's counter and streams
@@ -1021,27 +1082,37 @@ __global__ void __launch_bounds__(F_THREADS, 2)
 // no 128x8 instance: its halo box would be 272 cells wide, past the 256 a
 // TMA box allows.
 struct StreamShape {
-    int w, h, hx;
+    int w, h, hx, threads;
     size_t smem;
     const void* kern;
 };
-template <typename T, int S>
+template <typename T, int S, bool TAIL = false>
 static StreamShape stream_shape_t() {
     using TL = Tile<T, S>;
     static_assert(TL::HX <= 256 && TL::H + 2 <= 256, "TMA box dimensions are at most 256");
-    return StreamShape{TL::W, TL::H, TL::HX, TL::SMEM, (const void*)k_stream<T, S>};
+    return StreamShape{TL::W, TL::H, TL::HX, TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS, TL::SMEM,
+                       (const void*)k_stream<T, S, TAIL>};
 }
 static bool shape_valid(bool f16, int S) { return S >= 0 && S < kTileShapes && !(f16 && S == 1); }
-static StreamShape stream_shape(bool f16, int S) {
+// tail: the instance with tail warps (FP32 storage only)
+static StreamShape stream_shape(bool f16, int S, bool tail = false) {
     if (f16) return S == 2 ? stream_shape_t<__half, 2>() : stream_shape_t<__half, 0>();
+    if (tail)
+        return S == 1 ? stream_shape_t<float, 1, true>()
+                      : (S == 2 ? stream_shape_t<float, 2, true>() : stream_shape_t<float, 0, true>());
     return S == 1 ? stream_shape_t<float, 1>() : (S == 2 ? stream_shape_t<float, 2>() : stream_shape_t<float, 0>());
 }
 template <typename T>
-static void launch_stream(int S, int grid, cudaStream_t st, const CUtensorMap& th, const CUtensorMap& to,
+static void launch_stream(int S, bool tail, int grid, cudaStream_t st, const CUtensorMap& th, const CUtensorMap& to,
                           const StepArgs& a, const FusedDev& f, int j) {
     if constexpr (sizeof(T) == 2) {
         if (S == 2) k_stream<T, 2><<<grid, F_THREADS, Tile<T, 2>::SMEM, st>>>(th, to, a, f, j);
         else k_stream<T, 0><<<grid, F_THREADS, Tile<T, 0>::SMEM, st>>>(th, to, a, f, j);
+    } else if (tail) {
+        constexpr int TT = F_THREADS + 32 * kTailWarps;
+        if (S == 1) k_stream<T, 1, true><<<grid, TT, Tile<T, 1>::SMEM, st>>>(th, to, a, f, j);
+        else if (S == 2) k_stream<T, 2, true><<<grid, TT, Tile<T, 2>::SMEM, st>>>(th, to, a, f, j);
+        else k_stream<T, 0, true><<<grid, TT, Tile<T, 0>::SMEM, st>>>(th, to, a, f, j);
     } else {
         if (S == 1) k_stream<T, 1><<<grid, F_THREADS, Tile<T, 1>::SMEM, st>>>(th, to, a, f, j);
         else if (S == 2) k_stream<T, 2><<<grid, F_THREADS, Tile<T, 2>::SMEM, st>>>(th, to, a, f, j);
@@ -1344,6 +1415,7 @@ struct Engine::Impl {
     FusedDev fdev{};
     DBuf<int4> f_offs;
     DBuf<int> f_work;
+    DBuf<unsigned long long> f_tail;  // tail-warp counters, one per step of a chunk
     // compact work lists of the streaming kernel (FIXED scheme), one per plan
     struct PlanItems {
         std::array<int64_t, 7> key{{-1, -1, -1, -1, -1, -1, -1}};
@@ -1364,8 +1436,9 @@ struct Engine::Impl {
         int per_sm, dz;
         bool beside;  // boundary and PML pressure kernels beside the streaming kernel
         int shape;
+        bool tail;    // boundary and PML pressure work in the streaming kernel's tail warps
     };
-    Plan plan{0, 0, false, 0};
+    Plan plan{0, 0, false, 0, false};
     std::vector<Plan> tune_cands;
     std::vector<float> tune_ms;
     size_t tune_next = 0;
@@ -1375,7 +1448,7 @@ struct Engine::Impl {
     cudaEvent_t tev0 = nullptr, tev1 = nullptr;
     bool tune_active() const { return use_fused() && prm.graphs && !prm.profile && !tuned; }
     void apply_plan(int id) {
-        plan = id == 0 ? Plan{0, 0, false, 0} : tune_cands[(size_t)id - 1];
+        plan = id == 0 ? Plan{0, 0, false, 0, false} : tune_cands[(size_t)id - 1];
         plan_id = id;
         fused_dirty = true;
         build_fused();
@@ -1394,9 +1467,9 @@ struct Engine::Impl {
     }
     // a plan fixed by afd_set_plan: the only candidate, tuning off
     bool forced = false;
-    Plan forced_plan{0, 0, false, 0};
+    Plan forced_plan{0, 0, false, 0, false};
     // resident blocks per SM that fit and the z-chunk depth rule of a shape
-    void shape_limits(int shape, int* per_sm_max, int* dz_rule);
+    void shape_limits(int shape, bool tail, int* per_sm_max, int* dz_rule);
     void make_candidates() {
         tune_cands.clear();
         if (forced) {
@@ -1407,26 +1480,33 @@ struct Engine::Impl {
             tune_gen = model_gen;
             return;
         }
-        auto add = [&](int ps, int d, bool bs, int sh) {
+        auto add = [&](int ps, int d, bool bs, int sh, bool tl) {
             if (ps < 1 || d < 8) return;
             for (const Plan& q : tune_cands)
-                if (q.per_sm == ps && q.dz == d && q.beside == bs && q.shape == sh) return;
-            tune_cands.push_back(Plan{ps, d, bs, sh});
+                if (q.per_sm == ps && q.dz == d && q.beside == bs && q.shape == sh && q.tail == tl) return;
+            tune_cands.push_back(Plan{ps, d, bs, sh, tl});
         };
         for (int sh = 0; sh < kTileShapes; ++sh) {
             if (!shape_valid(f16(), sh)) continue;
             int ps = 0, rule = 0;
-            shape_limits(sh, &ps, &rule);
-            add(ps, rule, false, sh);
-            if (sh == 0) add(ps, rule / 2, false, sh);
-            add(ps, rule / 4, false, sh);
-            // the plans with the boundary and PML kernels beside the streaming
-            // kernel are offered for FP32 storage only: with FP16 storage they
-            // gave results that differed from the serial order and between
-            // runs (16-member batch), so FP16 runs keep the serial order
-            if (sh == 0 && owned.ptr && !ref() && !f16()) {
-                add(ps, rule, true, sh);
-                add(ps - 1, rule, true, sh);
+            shape_limits(sh, false, &ps, &rule);
+            add(ps, rule, false, sh, false);
+            if (sh == 0) add(ps, rule / 2, false, sh, false);
+            add(ps, rule / 4, false, sh, false);
+            if (owned.ptr && !ref() && !f16()) {
+                // FP32 storage: the boundary and PML pressure work in the
+                // streaming kernel's tail warps, and (64x16 tile) in kernels
+                // beside it; FP16 runs keep the serial order (their beside
+                // plans differed between runs before the scale slots were
+                // read through L2, and are slower)
+                int pt = 0, rt = 0;
+                shape_limits(sh, true, &pt, &rt);
+                add(pt, rt, false, sh, true);
+                add(pt, rt / 4, false, sh, true);
+                if (sh == 0) {
+                    add(ps, rule, true, sh, false);
+                    add(ps - 1, rule, true, sh, false);
+                }
             }
         }
         tune_ms.assign(tune_cands.size(), 0.0f);
@@ -1521,6 +1601,12 @@ struct Engine::Impl {
     // beside the streaming kernel (which skips the cells they own)
     bool lists_beside() const {
         return plan.beside && !ref() && use_fused() && prm.graphs && !prm.profile && owned.ptr;
+    }
+    // FIXED scheme, FP32 storage, graphs: the boundary and PML pressure
+    // updates run in the streaming kernel's tail warps
+    bool tail_active() const {
+        return plan.tail && !plan.beside && !ref() && !f16() && use_fused() && prm.graphs && !prm.profile &&
+               owned.ptr;
     }
     // (FT_X x FT_Y tile, plane) of a cell, in tile-major order
     int64_t tile_key(int x, int y, int z) const {
@@ -1685,11 +1771,11 @@ static int chunk_rule(int64_t tiles, int nz, int64_t resident) {
     return dz;
 }
 
-void Engine::Impl::shape_limits(int shape, int* per_sm_max, int* dz_rule) {
-    const StreamShape sh = stream_shape(f16(), shape);
+void Engine::Impl::shape_limits(int shape, bool tail, int* per_sm_max, int* dz_rule) {
+    const StreamShape sh = stream_shape(f16(), shape, tail);
     int per_sm = 0, sms = 0;
     CK(cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sh.kern, F_THREADS, sh.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sh.kern, sh.threads, sh.smem));
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     per_sm = std::max(per_sm, 1);
     const int64_t tiles = (int64_t)((nx + sh.w - 1) / sh.w) * ((ny + sh.h - 1) / sh.h) * prm.batch;
@@ -1703,7 +1789,7 @@ void Engine::Impl::build_fused() {
     FusedDev& F = fdev;
     F = FusedDev{};
     if (!shape_valid(f16(), plan.shape)) plan.shape = 0;
-    const StreamShape sh = stream_shape(f16(), plan.shape);
+    const StreamShape sh = stream_shape(f16(), plan.shape, tail_active());
     tile_w = sh.w;
     tile_h = sh.h;
     tiles_x = (nx + sh.w - 1) / sh.w;
@@ -1713,15 +1799,17 @@ void Engine::Impl::build_fused() {
     F.tiles_y = tiles_y;
     int per_sm = 0;
     CK(cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sh.kern, F_THREADS, sh.smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sh.kern, sh.threads, sh.smem));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     max_per_sm = std::max(per_sm, 1);
     if (plan.per_sm > 0) per_sm = std::min(per_sm, plan.per_sm);
     stream_per_sm = std::max(per_sm, 1);
     const int64_t resident = (int64_t)stream_per_sm * sms;
-    F.owned = lists_beside() ? owned.ptr : nullptr;
+    F.owned = lists_beside() || tail_active() ? owned.ptr : nullptr;
     F.owned_wpr = (int32_t)(pitch / 32);
+    if (!f_tail.ptr) f_tail.alloc(256);
+    F.tail = f_tail.ptr;
     const int64_t tiles = (int64_t)tiles_x * tiles_y * prm.batch;
     int dz = chunk_rule(tiles, nz, resident);
     rule_dz = dz;
@@ -2143,8 +2231,9 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         CK(cudaEventRecord(ev_pool[ev_kind.size() - 1].second, stream));
     };
     const dim3 blk(64, 4, 1);
+    const bool tail = tail_active() && step_phase == 0;
     auto stream_launch = [&](cudaStream_t st) {
-        launch_stream<T>(plan.shape, fused_grid, st, tm_halo, tm_own, a, fdev, j);
+        launch_stream<T>(plan.shape, tail, fused_grid, st, tm_halo, tm_own, a, fdev, j);
         ++launches;
     };
     // a split step (z-slab runs): phase 1 runs the interior, boundary and
@@ -2213,8 +2302,8 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         // auxiliary fields, so they run side by side; the auxiliary updates
         // (one per axis, disjoint outputs) follow once both are done.
         std::vector<std::function<void(cudaStream_t)>> g1, g2;
-        if (a.lrs.n > 0) g1.push_back(lrs_launch);
-        g1.push_back(pml_p_launch);
+        if (a.lrs.n > 0 && !tail) g1.push_back(lrs_launch);
+        if (!tail) g1.push_back(pml_p_launch);
         if (src_beside_aux && (a.src.n > 0 || a.rcv.n > 0)) {
             // queued first: its one block then starts at once instead of
             // waiting for the auxiliary updates' blocks to be dispatched
@@ -2225,7 +2314,7 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
         run_side_by_side(g1);
         run_side_by_side(g2);
     } else {
-        if (a.lrs.n > 0 && phA) {
+        if (a.lrs.n > 0 && phA && !tail) {
             begin(KK_LRS);
             lrs_launch(stream);
             end();
@@ -2277,6 +2366,7 @@ cudaGraphExec_t Engine::Impl::graph_for(int64_t n) {
     const int64_t saved = launches;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
+    if (tail_active()) CK(cudaMemsetAsync(f_tail.ptr, 0, (size_t)n * sizeof(unsigned long long), stream));
     for (int64_t j = 0; j < n; ++j) launch_step((int)j, false);
     k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
     CK(cudaStreamEndCapture(stream, &graph));
@@ -2320,11 +2410,12 @@ void Engine::Impl::collect_profile() {
 int64_t Engine::Impl::kernels_per_step() const {
     const StepArgs& a = args;
     int64_t k = 1;
-    if (a.lrs.n > 0) ++k;
+    const bool tail = tail_active();
+    if (a.lrs.n > 0 && !tail) ++k;
     if (a.pml.width > 0) {
         if (ref()) k += (nx > 4 && ny > 4 && nz > 4) ? 2 : 0;
         else if (a.pml.n_units > 0)
-            k += 2;
+            k += tail ? 1 : 2;
     }
     if (a.src.n > 0 || a.rcv.n > 0) ++k;
     if (cap_every > 0) ++k;
@@ -2502,10 +2593,10 @@ void Engine::set_plan(const afd_plan* p) {
     D.drop_graphs();
     D.plan_items.clear();
     D.forced = p != nullptr;
-    if (p) D.forced_plan = Impl::Plan{p->per_sm, p->dz, p->beside != 0, shape};
+    if (p) D.forced_plan = Impl::Plan{p->per_sm, p->dz, p->beside != 0, shape, p->tail != 0};
     D.tuned = false;
     D.tune_gen = -1;  // candidates are made again by the next run or prepare
-    D.plan = Impl::Plan{0, 0, false, 0};
+    D.plan = Impl::Plan{0, 0, false, 0, false};
     D.plan_id = 0;
     D.fused_dirty = true;
 }
@@ -3090,6 +3181,7 @@ void Engine::get_info(afd_info* info) {
     info->stream_blocks = D.fused_grid;
     info->stream_beside = D.lists_beside() ? 1 : 0;
     info->stream_per_sm = D.stream_per_sm;
+    info->stream_tail = D.tail_active() ? 1 : 0;
     info->tuned = D.tuned ? 1 : 0;
 }
 

@@ -68,6 +68,7 @@ struct FusedDev {
     int32_t n_items;
     const uint32_t* owned;  // null, or 1 bit per cell ([z][y][owned_wpr] words): cells not to store
     int32_t owned_wpr;
+    unsigned long long* tail;  // tail-warp work counters, one per step of a chunk
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {

@@ -293,7 +293,8 @@ typedef struct afd_info {
     int32_t tuned;               /* 1 once the online autotuner has chosen the plan */
     int32_t stream_beside;       /* 1: the plan runs the boundary and PML kernels beside the streaming kernel */
     int32_t stream_per_sm;       /* resident streaming blocks per SM of the plan */
-    int32_t reserved[5];
+    int32_t stream_tail;         /* 1: the plan does the boundary and PML pressure work in the streaming kernel */
+    int32_t reserved[4];
 } afd_info;
 int afd_get_info(afd_sim* s, afd_info* info);
 
@@ -321,7 +322,9 @@ typedef struct afd_plan {
     int32_t per_sm;          /* resident streaming blocks per SM */
     int32_t dz;              /* planes per z-chunk work item (1..1024) */
     int32_t beside;
-    int32_t reserved[3];
+    int32_t tail;            /* 1: the boundary and PML pressure work in the streaming kernel's tail warps
+                                (FIXED scheme, FP32 storage, CUDA graphs; ignored elsewhere) */
+    int32_t reserved[2];
 } afd_plan;
 
 /* Fixes the streaming plan of later runs and turns the online autotuner off

@@ -129,8 +129,8 @@ def c2_case():
 # rule's z-chunk depth (32) and a quarter of it, the boundary/PML kernels
 # beside the streaming kernel, and the other two tile shapes
 @pytest.mark.parametrize("plan", [dict(dz=8), dict(dz=32), dict(beside=True), dict(tile=(128, 8), dz=8),
-                                  dict(tile=(32, 32), dz=8)],
-                         ids=["dz8", "dz32", "beside", "tile128x8", "tile32x32"])
+                                  dict(tile=(32, 32), dz=8), dict(tail=True), dict(tail=True, tile=(128, 8), dz=8)],
+                         ids=["dz8", "dz32", "beside", "tile128x8", "tile32x32", "tail", "tail128x8"])
 def test_c2_benchmark_workload_full_size(pkg, c2_case, plan):
     cfg, steps, want, wfield, w64, f64 = c2_case
     sim = _sim(pkg, cfg, plan=plan)
@@ -140,6 +140,7 @@ def test_c2_benchmark_workload_full_size(pkg, c2_case, plan):
     assert info.tile_z == plan.get("dz", info.tile_z)
     assert bool(info.stream_beside) == plan.get("beside", False)
     assert (info.tile_x, info.tile_y) == plan.get("tile", (64, 16))
+    assert bool(info.stream_tail) == plan.get("tail", False)
     got, field = sim.mics(), sim.field()
     sim.close()
     assert np.array_equal(got, want)

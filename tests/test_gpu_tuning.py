@@ -90,6 +90,7 @@ def test_every_plan_twice_equals_serial_run(pkg, storage):
         if plan is not None:
             assert bool(info.stream_beside) == plan.get("beside", False)
             assert (info.tile_x, info.tile_y) == plan.get("tile", (64 * (2 if storage else 1), 16))
+            assert bool(info.stream_tail) == plan.get("tail", False)
         out = np.stack([sim.mics(batch=m) for m in range(16)]), sim.field(batch=7)
         sim.close()
         return out
@@ -98,7 +99,7 @@ def test_every_plan_twice_equals_serial_run(pkg, storage):
     wide = 2 if storage else 1  # FP16 storage doubles the tile width in cells
     plans = [dict(), dict(dz=8), dict(beside=True), dict(beside=True, per_sm=1), dict(tile=(32 * wide, 32))]
     if not storage:
-        plans.append(dict(tile=(128, 8), dz=8))
+        plans += [dict(tile=(128, 8), dz=8), dict(tail=True), dict(tail=True, tile=(128, 8), dz=8)]
     for plan in plans:
         for _ in range(2):
             got = run(1, plan)
