@@ -1602,12 +1602,9 @@ struct Engine::Impl {
     bool lists_beside() const {
         return plan.beside && !ref() && use_fused() && prm.graphs && !prm.profile && owned.ptr;
     }
-    // FIXED scheme, FP32 storage, graphs: the boundary and PML pressure
-    // updates run in the streaming kernel's tail warps
-    bool tail_active() const {
-        return plan.tail && !plan.beside && !ref() && !f16() && use_fused() && prm.graphs && !prm.profile &&
-               owned.ptr;
-    }
+    // FIXED scheme, FP32 storage: the boundary and PML pressure updates run
+    // in the streaming kernel's tail warps (with or without graphs)
+    bool tail_active() const { return plan.tail && !plan.beside && !ref() && !f16() && use_fused() && owned.ptr; }
     // (FT_X x FT_Y tile, plane) of a cell, in tile-major order
     int64_t tile_key(int x, int y, int z) const {
         return ((int64_t)(y / FT_Y) * ((nx + FT_X - 1) / FT_X) + x / FT_X) * nz + z;
@@ -2333,7 +2330,7 @@ void Engine::Impl::launch_step_t(int j, bool profile) {
                     launches += 2;
                 }
             } else if (a.pml.n_units > 0) {
-                if (phA) {
+                if (phA && !tail) {
                     begin(KK_PML_P);
                     pml_p_launch(stream);
                     end();
@@ -2387,6 +2384,7 @@ void Engine::Impl::run_chunk(int64_t n) {
         launch_step_count_only(n);
     } else {
         if (use_fused()) CK(cudaMemsetAsync(f_work.ptr, 0, (size_t)n * sizeof(int), stream));
+        if (tail_active()) CK(cudaMemsetAsync(f_tail.ptr, 0, (size_t)n * sizeof(unsigned long long), stream));
         for (int64_t j = 0; j < n; ++j) launch_step((int)j, profile);
         k_advance<<<1, 1, 0, stream>>>(d_step.ptr, (int)n);
         ++launches;
