@@ -133,3 +133,36 @@ def test_training_fits_a_smooth_target(pkg):
     assert loss < 0.1 * first
     assert err < 0.45
     m.close()
+
+
+def test_split_gemm_reaches_fp32_accuracy(pkg):
+    """The readout's normal equations use the tcgen05 GEMM on BF16 value and
+    remainder parts: the three-product sum matches the FP64 product of the
+    FP32 operands to FP32-level accuracy (one BF16 product alone is ~1e-3)."""
+    import torch
+    import ancfield_b200.surrogate_workflow as SW
+    g = torch.Generator(device="cpu").manual_seed(3)
+    a = torch.randn(300, 700, generator=g).cuda()
+    b = torch.randn(260, 700, generator=g).cuda()
+    c = SW.gemm_split(pkg, a, b)
+    want = a.double() @ b.double().t()
+    err = float((c.double() - want).norm() / want.norm())
+    assert c.shape == (300, 260)
+    assert err < 1e-5, err
+
+
+def test_field_readout_gain_over_fdtd(pkg):
+    """The learned readout (random Fourier features of the receiver position,
+    output layer fitted through the normal equations on the tcgen05 GEMM)
+    against the FDTD at receiver positions the generating run did not train
+    on: the fraction of pairs within 1 % relative L2, the IRs/s with FDTD
+    fallback for the pairs whose predicted error exceeds 1 %, and the gain
+    over answering every pair with the FDTD alone."""
+    import ancfield_b200.surrogate_workflow as SW
+    r = SW.run_field_readout(pkg, n_sets=1, n_src=4, n_query=64, n_val=64, plain=False)
+    print({k: r[k] for k in ("query_rel_l2", "within_bound", "accepted", "accepted_but_over_bound",
+                             "fallback_runs", "irs_per_s", "gain_over_fdtd")})
+    assert r["within_bound"] >= 0.5
+    # accepted pairs whose true error exceeds the bound: at most 2 %
+    assert r["accepted_but_over_bound"] <= 0.02 * r["query_pairs"]
+    assert r["gain_over_fdtd"] > 1.0

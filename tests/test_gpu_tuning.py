@@ -19,7 +19,7 @@ def test_tuned_run_equals_serial_run(pkg, storage):
     vox = W.close_gaps(vox)
     nz, ny, nx = vox.shape
     ksi = W.ksi_arrays((nx, ny, nz), 8, W.FACE_ZP, kmax=6000.0)
-    sig = W.gaussian_pulse(2400, 32000.0)
+    sig = W.gaussian_pulse(3600, 32000.0)
     out = []
     for graphs in (1, 0):
         sim = pkg.Simulation(mode=1, graphs=graphs, storage=storage)
@@ -28,7 +28,7 @@ def test_tuned_run_equals_serial_run(pkg, storage):
         sim.AddSourceCell((30, 30, 20), sig)
         for r in [(50, 40, 30), (80, 20, 55), (10, 60, 10)]:
             sim.AddMicCell(r)
-        sim.Run(2201)
+        sim.Run(3401)
         sim.Run(199)
         info = sim.info()
         assert bool(info.tuned) == bool(graphs)
@@ -45,7 +45,7 @@ def test_tuned_batch_equals_serial_run(pkg, storage):
     half-depth candidate too, and a tuned run that tries every candidate
     equals the serial run without graphs bit for bit, member by member."""
     W = pkg.workloads
-    cfg = W.config_c3(steps=2200)
+    cfg = W.config_c3(steps=3400)
     out = []
     for graphs in (1, 0):
         sim = pkg.Simulation(mode=1, dx=cfg.dx, c=cfg.c, dt=cfg.dt, batch=16, graphs=graphs, storage=storage)
@@ -56,7 +56,7 @@ def test_tuned_batch_equals_serial_run(pkg, storage):
                 sim.AddSourceCell(cell, sig, batch=m)
         for r in cfg.receivers:
             sim.AddMicCell(r)
-        sim.Run(2200)
+        sim.Run(3400)
         assert bool(sim.info().tuned) == bool(graphs)
         out.append(np.stack([sim.mics(batch=m) for m in range(16)]))
         sim.close()
