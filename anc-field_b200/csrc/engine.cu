@@ -1453,12 +1453,11 @@ struct Engine::Impl {
         fused_dirty = true;
         build_fused();
     }
-    // candidates: for each tile shape the streaming kernel alone with all
-    // resident blocks per SM and z-chunk depth {rule, rule / 4} (and rule / 2
-    // for the 64x16 tile), or (FP32 storage, 64x16 tile) beside the boundary
-    // and PML kernels with {all, all - 1} blocks per SM; every candidate gives
-    // the results of the serial order. Made once per model and grid (the plan
-    // then restarts from the default).
+    // candidates: for each tile shape the streaming kernel with all resident
+    // blocks per SM and z-chunk depth {rule, rule / 4} (and rule / 2 for the
+    // 64x16 tile), followed by the boundary and PML kernels; every candidate
+    // gives the results of the serial order. Made once per model and grid
+    // (the plan then restarts from the default).
     void ensure_candidates() {
         if (use_fused() && tune_gen != model_gen) {
             make_candidates();
@@ -1493,21 +1492,9 @@ struct Engine::Impl {
             add(ps, rule, false, sh, false);
             if (sh == 0) add(ps, rule / 2, false, sh, false);
             add(ps, rule / 4, false, sh, false);
-            if (owned.ptr && !ref() && !f16()) {
-                // FP32 storage: the boundary and PML pressure work in the
-                // streaming kernel's tail warps, and (64x16 tile) in kernels
-                // beside it; FP16 runs keep the serial order (their beside
-                // plans differed between runs before the scale slots were
-                // read through L2, and are slower)
-                int pt = 0, rt = 0;
-                shape_limits(sh, true, &pt, &rt);
-                add(pt, rt, false, sh, true);
-                add(pt, rt / 4, false, sh, true);
-                if (sh == 0) {
-                    add(ps, rule, true, sh, false);
-                    add(ps - 1, rule, true, sh, false);
-                }
-            }
+            // the beside and tail-warp orders (afd_set_plan) give the same
+            // results but measured slower on every workload here, so the
+            // tuner does not spend chunks on them
         }
         tune_ms.assign(tune_cands.size(), 0.0f);
         tune_next = 0;

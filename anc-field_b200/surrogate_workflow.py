@@ -350,7 +350,7 @@ class FieldReadout:
     solved in FP64. One readout serves every (wall set, source) recorded at
     the same receiver positions: their IRs are the columns of Y."""
 
-    def __init__(self, pkg, n_feat=4096, sigma=6.0, ridge=1e-6, seed=0):
+    def __init__(self, pkg, n_feat=4096, sigma=6.0, ridge=1e-4, seed=0):
         import torch
         self.pkg = pkg
         g = torch.Generator(device="cpu").manual_seed(seed)
@@ -373,9 +373,21 @@ class FieldReadout:
         y = torch.as_tensor(y, dtype=torch.float32, device="cuda")
         gram = gemm_split(self.pkg, pt, pt).double()        # [D, D]
         rhs = gemm_split(self.pkg, pt, y.t().contiguous()).double()  # [D, L]
-        lam = self.ridge * torch.trace(gram) / self.n_feat
-        gram.diagonal().add_(lam)
-        L = torch.linalg.cholesky(gram)
+        # ridge relative to the mean diagonal; the Gram matrix of smooth
+        # random features is numerically singular, so a ridge too small for
+        # the factorisation is raised tenfold until it factors
+        mean_diag = float(torch.trace(gram)) / self.n_feat
+        ridge = self.ridge
+        while True:
+            a = gram.clone()
+            a.diagonal().add_(ridge * mean_diag)
+            L, info = torch.linalg.cholesky_ex(a)
+            if int(info) == 0:
+                break
+            ridge *= 10.0
+            if ridge > 1.0:
+                raise RuntimeError("readout normal equations do not factor")
+        self.ridge_used = ridge
         self.beta = torch.cholesky_solve(rhs, L).float()    # [D, L]
         self.beta_t = self.beta.t().contiguous()            # [L, D]
         return self
@@ -393,21 +405,10 @@ def field_irs(pkg, g, src_cells, rcv_cells):
     return torch.from_numpy(irs).cuda(), wall
 
 
-def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, seed=21, n_feat=4096,
-                      sigma=6.0, grid_h=GRID_H, plain=True):
-    """The learned readout against the FDTD for receiver positions that the
-    generating runs did not record as training data (new positions, the
-    runs' own wall sets and sources; the query and validation receivers are
-    recorded in the same runs as the FDTD answer). Per wall set: one batched
-    FDTD run of n_src sources with the receiver grid, n_query query and
-    n_val validation receivers. The readout is fitted on the grid; a
-    committee of two readouts fitted on the two halves of the grid gives
-    each pair a predicted error (their disagreement, calibrated on the
-    validation receivers), and a pair whose predicted error exceeds `bound`
-    falls back to the FDTD: one plain single-source run per (wall set,
-    source) that has such a pair. Without the readout every query pair
-    needs the FDTD: one batched run per wall set. Reports errors, the
-    fraction within the bound, IRs/s of each path and the gain."""
+def field_data(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, seed=21, grid_h=GRID_H):
+    """The batched FDTD runs behind the readout: per wall set one run of
+    n_src sources whose receivers are the grid, n_query query and n_val
+    validation positions. IRs stay on the device, [n_sets, n_src, n, L]."""
     import torch
     rng = np.random.default_rng(seed)
     grid = receiver_grid(grid_h)
@@ -421,17 +422,44 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     for w in range(n_sets):
         irs, wall = field_irs(pkg, gsets[w], srcs[w], rcv)
         fd_s.append(wall)
-        Y_grid.append(irs[:, :ng])            # [S, G, L]
+        Y_grid.append(irs[:, :ng])
         Y_q.append(irs[:, ng:ng + n_query])
         Y_v.append(irs[:, ng + n_query:])
         del irs
-    # columns: (wall set, source, sample)
+    # grid IRs as columns (wall set, source, sample)
     yg = torch.cat([t.permute(1, 0, 2).reshape(ng, -1) for t in Y_grid], dim=1)
+    return {"grid": grid, "q_cells": q_cells, "v_cells": v_cells, "yg": yg, "yq": torch.stack(Y_q),
+            "yv": torch.stack(Y_v), "fd_s": fd_s, "gsets": gsets, "srcs": srcs, "n_sets": n_sets, "n_src": n_src,
+            "grid_h": grid_h, "seed": seed}
+
+
+def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, seed=21, n_feat=4096,
+                      sigma=4.0, ridge=1e-4, grid_h=GRID_H, plain=True, data=None):
+    """The learned readout against the FDTD for receiver positions that the
+    generating runs did not record as training data (new positions, the
+    runs' own wall sets and sources; the query and validation receivers are
+    recorded in the same runs as the FDTD answer). Per wall set: one batched
+    FDTD run of n_src sources with the receiver grid, n_query query and n_val
+    validation receivers (field_data; `data` reuses earlier runs). The
+    readout is fitted on the grid; a committee of two readouts fitted on the
+    two halves of the grid gives each pair a predicted error (their
+    disagreement, calibrated on the validation receivers), and a pair whose
+    predicted error exceeds `bound` falls back to the FDTD: one plain
+    single-source run per (wall set, source) that has such a pair. Without
+    the readout every query pair needs the FDTD: one batched run per wall
+    set. Reports errors, the fraction within the bound, IRs/s of each path
+    and the gain."""
+    import torch
+    d = data or field_data(pkg, n_sets, n_src, n_query, n_val, seed, grid_h)
+    n_sets, n_src = d["n_sets"], d["n_src"]
+    grid, q_cells, v_cells = d["grid"], d["q_cells"], d["v_cells"]
+    n_query, n_val, ng = len(q_cells), len(v_cells), len(grid)
+    yg, fd_s = d["yg"], d["fd_s"]
     scale = float(yg.pow(2).mean().sqrt())
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    full = FieldReadout(pkg, n_feat=n_feat, sigma=sigma, seed=seed).fit(grid, yg / scale)
-    half = [FieldReadout(pkg, n_feat=n_feat, sigma=sigma, seed=seed).fit(grid[k::2], yg[k::2] / scale)
+    full = FieldReadout(pkg, n_feat=n_feat, sigma=sigma, ridge=ridge, seed=seed).fit(grid, yg / scale)
+    half = [FieldReadout(pkg, n_feat=n_feat, sigma=sigma, ridge=ridge, seed=seed).fit(grid[k::2], yg[k::2] / scale)
             for k in range(2)]
     torch.cuda.synchronize()
     t_fit = time.perf_counter() - t0
@@ -443,12 +471,12 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     def rel(a, b):
         return ((a - b).norm(dim=-1) / b.norm(dim=-1).clamp_min(1e-30)).cpu().numpy()
 
-    yv = torch.stack(Y_v) / scale
+    yv = d["yv"] / scale
     pv = split_pairs(full.predict(v_cells), n_val)
     dv = rel(split_pairs(half[0].predict(v_cells), n_val), split_pairs(half[1].predict(v_cells), n_val))
     ev = rel(pv, yv)
     calib = float(np.median(ev / np.maximum(dv, 1e-12)))  # true error per unit of committee disagreement
-    yq = torch.stack(Y_q) / scale
+    yq = d["yq"] / scale
     full.predict(q_cells[:8])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -462,7 +490,7 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     runs_needed = int((~accept).any(axis=2).sum())
     t_plain = None
     if plain:
-        _, t_plain = plain_irs(pkg, gsets[0], srcs[0][0], q_cells[:16])
+        _, t_plain = plain_irs(pkg, d["gsets"][0], d["srcs"][0][0], q_cells[:16])
     t_single = t_plain if t_plain is not None else float(np.mean(fd_s)) / n_src
     n_pairs = n_sets * n_src * n_query
     t_fallback = runs_needed * t_single
@@ -470,9 +498,9 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     irs_fdtd = n_pairs / fdtd_alone_s
     irs_sur = n_pairs / (t_pred + t_fallback)
     return {
-        "wall_sets": n_sets, "sources_per_set": n_src, "grid_receivers": ng, "grid_spacing_m": grid_h,
+        "wall_sets": n_sets, "sources_per_set": n_src, "grid_receivers": ng, "grid_spacing_m": d["grid_h"],
         "query_pairs": n_pairs, "validation_pairs": n_sets * n_src * n_val, "features": n_feat,
-        "sigma_rad_per_m": sigma, "fit_s": t_fit, "fdtd_run_s": fd_s,
+        "sigma_rad_per_m": sigma, "ridge": full.ridge_used, "fit_s": t_fit, "fdtd_run_s": fd_s,
         "query_rel_l2": {"median": float(np.median(eq)), "p90": float(np.percentile(eq, 90)),
                          "max": float(eq.max())},
         "validation_median_rel_l2": float(np.median(ev)),
