@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="c3: shard the sources over the job's ranks and gather the receivers (the default "
                          "when the job has more than one rank)")
+    ap.add_argument("--plan", default=None,
+                    help="WxH[:DZ]: force the streaming plan (tile W x H cells, z-chunk depth DZ) instead of "
+                         "letting the autotuner choose (profiling captures of one plan)")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="field storage: fp32, or fp16 levels with per-level power-of-two scales")
     return ap.parse_args()
@@ -573,6 +576,10 @@ def main():
         return sim
 
     sim = make_sim()
+    if args.plan:
+        tile, _, dz = args.plan.partition(":")
+        tw, th = (int(v) for v in tile.split("x"))
+        sim.set_plan(tile=(tw, th), dz=int(dz) if dz else 0)
     K, Wm = args.steps, max(args.warmup, 3)
     if "device" not in legs:
         legs.add("device")
