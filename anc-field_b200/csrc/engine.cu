@@ -885,6 +885,11 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
     const int lane = tid & 31;
     const int cx = (tid % TL::TPR) * TL::CPT, cy = tid / TL::TPR;
     const float L2 = a.lambda2, CI = a.cint;
+    // FP16: the level scales of the current member, loaded again only when
+    // a work item of another member comes (items of one member are
+    // consecutive in the list), so the L2 load is off most items' path
+    int sc_b = -1;
+    StepScales sc_cached{};
     uint32_t k = 0;
     while (true) {
         if (!mbar_wait(&full[k % F_STAGES], (k / F_STAGES) & 1)) {
@@ -954,7 +959,11 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
             // registers from plane to plane: each plane loads and converts
             // only z+1, y+-1 and p^{n-1}. The update runs on stored values
             // of level g-1 (scale s_cur) and is rescaled once at the end.
-            const StepScales sc = step_scales(a.f16, it.b, g);
+            if (it.b != sc_b) {
+                sc_cached = step_scales(a.f16, it.b, g);
+                sc_b = it.b;
+            }
+            const StepScales sc = sc_cached;
             const float rc = sc.s_new * sc.inv_cur, ro = sc.s_cur * sc.inv_old;
             uint32_t vmask[4];
 #pragma unroll
@@ -2569,6 +2578,8 @@ void Engine::set_plan(const afd_plan* p) {
         if (shape < 0)
             throw Error(AFD_ERR_ARG, D.f16() ? "unsupported streaming tile (FP16 storage: 128x16 or 64x32)"
                                              : "unsupported streaming tile (64x16, 128x8 or 32x32)");
+        if (p->beside && D.f16())
+            throw Error(AFD_ERR_ARG, "beside plans are FP32-only (with FP16 storage they differed between runs)");
         if (p->per_sm < 0 || p->per_sm > 32) throw Error(AFD_ERR_ARG, "per_sm out of range (0..32)");
         if (p->dz < 0 || p->dz > 1024) throw Error(AFD_ERR_ARG, "dz out of range (0..1024)");
     }

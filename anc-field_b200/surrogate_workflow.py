@@ -350,19 +350,30 @@ class FieldReadout:
     solved in FP64. One readout serves every (wall set, source) recorded at
     the same receiver positions: their IRs are the columns of Y."""
 
-    def __init__(self, pkg, n_feat=4096, sigma=6.0, ridge=1e-4, seed=0):
+    def __init__(self, pkg, n_feat=4096, sigma=6.0, ridge=1e-4, seed=0, source=None):
         import torch
         self.pkg = pkg
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.W = (torch.randn(3, n_feat, generator=g, dtype=torch.float64) * sigma).float().cuda()
         self.c = (torch.rand(n_feat, generator=g, dtype=torch.float64) * 2 * math.pi).float().cuda()
-        self.n_feat, self.ridge = n_feat, ridge
+        self.base, self.ridge = n_feat, ridge
+        # a readout of one source can carry the direct sound's 1/R near the
+        # source: the features again, weighted by R0 / max(R, R_MIN)
+        self.source = None if source is None else np.asarray(source, np.float64) * DX
+        self.n_feat = n_feat * (2 if source is not None else 1)
         self.beta = None
+
+    R0, R_MIN = 0.5, 0.1  # m
 
     def features(self, cells):
         import torch
         r = torch.as_tensor(np.asarray(cells, np.float64) * DX, dtype=torch.float32, device="cuda")
-        return math.sqrt(2.0 / self.n_feat) * torch.cos(r @ self.W + self.c)
+        phi = math.sqrt(2.0 / self.base) * torch.cos(r @ self.W + self.c)
+        if self.source is None:
+            return phi
+        d = np.linalg.norm(np.asarray(cells, np.float64) * DX - self.source, axis=1)
+        w = torch.as_tensor(self.R0 / np.maximum(d, self.R_MIN), dtype=torch.float32, device="cuda")
+        return torch.cat([phi, phi * w[:, None]], dim=1).contiguous()
 
     def fit(self, cells, y):
         """cells [N, 3]; y [N, L] (device or host, FP32): one column block per
@@ -434,7 +445,7 @@ def field_data(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, seed=21, grid_h=GRI
 
 
 def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, seed=21, n_feat=4096,
-                      sigma=4.0, ridge=1e-4, grid_h=GRID_H, plain=True, data=None):
+                      sigma=4.0, ridge=1e-4, grid_h=GRID_H, plain=True, data=None, near=False):
     """The learned readout against the FDTD for receiver positions that the
     generating runs did not record as training data (new positions, the
     runs' own wall sets and sources; the query and validation receivers are
@@ -456,35 +467,53 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     n_query, n_val, ng = len(q_cells), len(v_cells), len(grid)
     yg, fd_s = d["yg"], d["fd_s"]
     scale = float(yg.pow(2).mean().sqrt())
+    ygs = yg / scale
+
+    def triple(cols, src):
+        def make():
+            return FieldReadout(pkg, n_feat=n_feat, sigma=sigma, ridge=ridge, seed=seed, source=src)
+        return (make().fit(grid, ygs[:, cols]), make().fit(grid[0::2], ygs[0::2, cols]),
+                make().fit(grid[1::2], ygs[1::2, cols]))
+
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    full = FieldReadout(pkg, n_feat=n_feat, sigma=sigma, ridge=ridge, seed=seed).fit(grid, yg / scale)
-    half = [FieldReadout(pkg, n_feat=n_feat, sigma=sigma, ridge=ridge, seed=seed).fit(grid[k::2], yg[k::2] / scale)
-            for k in range(2)]
+    if near:
+        # one readout per (wall set, source), with the source's 1/R features
+        models = [[triple(slice((w * n_src + k) * IR_LEN, (w * n_src + k + 1) * IR_LEN), d["srcs"][w][k])
+                   for k in range(n_src)] for w in range(n_sets)]
+    else:
+        models = triple(slice(None), None)  # one readout for every (wall set, source)
     torch.cuda.synchronize()
     t_fit = time.perf_counter() - t0
 
-    def split_pairs(pred, n):
-        # [n, n_sets * n_src * L] -> [n_sets, n_src, n, L]
-        return pred.reshape(n, n_sets, n_src, IR_LEN).permute(1, 2, 0, 3)
+    def predict(cells, which):
+        """[n_sets, n_src, n, L] predictions of readout `which` (0 full, 1, 2 halves)."""
+        n = len(cells)
+        if near:
+            return torch.stack([torch.stack([models[w][k][which].predict(cells) for k in range(n_src)])
+                                for w in range(n_sets)])
+        return models[which].predict(cells).reshape(n, n_sets, n_src, IR_LEN).permute(1, 2, 0, 3)
 
     def rel(a, b):
         return ((a - b).norm(dim=-1) / b.norm(dim=-1).clamp_min(1e-30)).cpu().numpy()
 
     yv = d["yv"] / scale
-    pv = split_pairs(full.predict(v_cells), n_val)
-    dv = rel(split_pairs(half[0].predict(v_cells), n_val), split_pairs(half[1].predict(v_cells), n_val))
+    pv = predict(v_cells, 0)
+    dv = rel(predict(v_cells, 1), predict(v_cells, 2))
     ev = rel(pv, yv)
     calib = float(np.median(ev / np.maximum(dv, 1e-12)))  # true error per unit of committee disagreement
     yq = d["yq"] / scale
-    full.predict(q_cells[:8])
+    predict(q_cells[:8], 0)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    pq = split_pairs(full.predict(q_cells), n_query)
-    dq = rel(split_pairs(half[0].predict(q_cells), n_query), split_pairs(half[1].predict(q_cells), n_query))
+    pq = predict(q_cells, 0)
+    dq = rel(predict(q_cells, 1), predict(q_cells, 2))
     torch.cuda.synchronize()
     t_pred = time.perf_counter() - t0
     eq = rel(pq, yq)                           # [n_sets, n_src, n_query]
+    dist = np.stack([np.stack([np.linalg.norm((q_cells - np.asarray(d["srcs"][w][k])) * DX, axis=1)
+                               for k in range(n_src)]) for w in range(n_sets)])
+    far = dist >= 0.5
     pe = calib * dq
     accept = pe <= bound
     runs_needed = int((~accept).any(axis=2).sum())
@@ -500,10 +529,13 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     return {
         "wall_sets": n_sets, "sources_per_set": n_src, "grid_receivers": ng, "grid_spacing_m": d["grid_h"],
         "query_pairs": n_pairs, "validation_pairs": n_sets * n_src * n_val, "features": n_feat,
-        "sigma_rad_per_m": sigma, "ridge": full.ridge_used, "fit_s": t_fit, "fdtd_run_s": fd_s,
+        "sigma_rad_per_m": sigma, "near_field_features": bool(near), "fit_s": t_fit, "fdtd_run_s": fd_s,
         "query_rel_l2": {"median": float(np.median(eq)), "p90": float(np.percentile(eq, 90)),
                          "max": float(eq.max())},
         "validation_median_rel_l2": float(np.median(ev)),
+        "query_rel_l2_beyond_half_metre": {"median": float(np.median(eq[far])) if far.any() else None,
+                                           "within_bound": float((eq[far] <= bound).mean()) if far.any() else None,
+                                           "pairs": int(far.sum())},
         "within_bound": float((eq <= bound).mean()), "accepted": float(accept.mean()),
         "accepted_but_over_bound": int((accept & (eq > bound)).sum()),
         "fallback_runs": runs_needed,

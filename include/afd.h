@@ -316,14 +316,16 @@ int afd_set_stream(afd_sim* s, void* stream);
  * the default: the 64x16 tile, as many resident blocks per SM as fit, the
  * z-chunk depth rule. beside = 1 runs the boundary and PML pressure kernels
  * beside the streaming kernel, which then skips their cells (FIXED scheme
- * with CUDA graphs only; ignored elsewhere). */
+ * with CUDA graphs; FP32 storage only: AFD_ERR_ARG with FP16 storage; ignored
+ * elsewhere). The autotuner tries neither the beside nor the tail order
+ * (both measured slower). */
 typedef struct afd_plan {
     int32_t tile_x, tile_y;  /* streaming tile in cells: 64x16, 128x8 or 32x32 (FP16 storage doubles x) */
     int32_t per_sm;          /* resident streaming blocks per SM */
     int32_t dz;              /* planes per z-chunk work item (1..1024) */
     int32_t beside;
     int32_t tail;            /* 1: the boundary and PML pressure work in the streaming kernel's tail warps
-                                (FIXED scheme, FP32 storage, CUDA graphs; ignored elsewhere) */
+                                (FIXED scheme, FP32 storage; ignored elsewhere) */
     int32_t reserved[2];
 } afd_plan;
 
