@@ -747,7 +747,8 @@ def e2e_leg(sim, cfg, K, interior, world, metric):
 # dominant kernel, from one ncu capture of that kernel on the full-size
 # workload (the ncu summary in profiles/ records the command), keyed by grid
 # and storage; the line reports it with traffic_source "ncu capture".
-MEASURED_TRAFFIC = {((512, 384, 320), "fp32", (64, 16), False): ("interior_stream", 740.42e6)}
+MEASURED_TRAFFIC = {((512, 384, 320), "fp32", (64, 16), False): ("interior_stream", 740.42e6),
+                    ((512, 384, 320), "fp32", (128, 8), False): ("interior_stream", 724.12e6)}
 
 
 def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0, traffic_key=None, plan=None, step_parts=None):
