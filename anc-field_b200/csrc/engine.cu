@@ -54,11 +54,19 @@ struct DBuf {
         if (count == 0) return;
         CK(cudaMalloc(&ptr, count * sizeof(T)));
         n = count;
-        if (zero) CK(cudaMemset(ptr, 0, count * sizeof(T)));
+        // the engine's streams are non-blocking and do not wait for the
+        // legacy stream the zeroing runs on: finished before return
+        if (zero) {
+            CK(cudaMemset(ptr, 0, count * sizeof(T)));
+            CK(cudaStreamSynchronize(cudaStreamLegacy));
+        }
     }
     void upload(const std::vector<T>& v) {
-        alloc(v.size());
-        if (!v.empty()) CK(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        alloc(v.size(), false);
+        if (v.empty()) return;
+        // a copy from pageable memory may return before its DMA lands
+        CK(cudaMemcpy(ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        CK(cudaStreamSynchronize(cudaStreamLegacy));
     }
 };
 
@@ -2443,6 +2451,7 @@ Engine::Engine(const afd_params& p) : d_(new Impl) {
     D.d_flag.alloc(1);
     D.d_energy.alloc(1);
     CK(cudaMemcpyToSymbol(c_group_mask, kGroupMask, sizeof(kGroupMask)));
+    CK(cudaStreamSynchronize(cudaStreamLegacy));  // before any launch on the non-blocking stream
     for (int k = 0; k < KK_COUNT; ++k) D.kstats.push_back(KernelStat{kKernelNames[k], 0, 0.0});
 }
 

@@ -178,7 +178,10 @@ struct Buf {
     }
     void alloc(size_t n) {
         LCK(cudaMalloc(&p, n * sizeof(T)));
+        // zeroed on the legacy stream, which the non-blocking work stream
+        // does not wait for: finished before return
         LCK(cudaMemset(p, 0, n * sizeof(T)));
+        LCK(cudaStreamSynchronize(cudaStreamLegacy));
     }
 };
 

@@ -618,7 +618,10 @@ struct Dev {
         n = count;
         if (count) {
             MCK(cudaMalloc(&p, count * sizeof(T)));
+            // the zeroing runs on the legacy stream, which the surrogate's
+            // non-blocking stream does not wait for: finished before return
             MCK(cudaMemset(p, 0, count * sizeof(T)));
+            MCK(cudaStreamSynchronize(cudaStreamLegacy));
         }
     }
 };
@@ -795,7 +798,8 @@ struct afd_mlp {
         std::vector<float> fb((size_t)p.n_in * p.n_freq);
         for (auto& v : fb) v = (float)(nd(rng) * p.fourier_sigma);
         fourier.alloc(fb.size());
-        MCK(cudaMemcpy(fourier.p, fb.data(), fb.size() * 4, cudaMemcpyHostToDevice));
+        MCK(cudaMemcpyAsync(fourier.p, fb.data(), fb.size() * 4, cudaMemcpyHostToDevice, stream));
+        MCK(cudaStreamSynchronize(stream));
         for (int l = 0; l < p.n_layers; ++l) {
             Layer* ly = new Layer;
             L.push_back(ly);
@@ -808,7 +812,8 @@ struct afd_mlp {
             std::uniform_real_distribution<double> ud(-a, a);
             for (auto& v : w) v = (float)ud(rng);
             ly->w.alloc(nw);
-            MCK(cudaMemcpy(ly->w.p, w.data(), nw * 4, cudaMemcpyHostToDevice));
+            MCK(cudaMemcpyAsync(ly->w.p, w.data(), nw * 4, cudaMemcpyHostToDevice, stream));
+            MCK(cudaStreamSynchronize(stream));
             ly->b.alloc(ly->out);
             ly->gw.alloc(nw);
             ly->gb.alloc(ly->out);
