@@ -445,7 +445,7 @@ def field_data(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, seed=21, grid_h=GRI
 
 
 def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, seed=21, n_feat=4096,
-                      sigma=2.0, ridge=1e-4, grid_h=GRID_H, plain=True, data=None, near=True, calib_q=0.9):
+                      sigma=2.0, ridge=1e-4, grid_h=GRID_H, plain=True, data=None, near=True, calib_q=0.8):
     """The learned readout against the FDTD for receiver positions that the
     generating runs did not record as training data (new positions, the
     runs' own wall sets and sources; the query and validation receivers are
@@ -459,10 +459,10 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     single-source run per (wall set, source) that has such a pair. Without
     the readout every query pair needs the FDTD: one batched run per wall
     set. That is the setting where every query position is known before the
-    runs ("queries_before_runs"); where query positions arrive after the runs
-    ("queries_after_runs"), the FDTD answers each new position with one
-    batched run of its wall set (every source), and the readout falls back
-    to such a run for a position with any rejected pair. The committee's
+    runs (the top-level gain); where query pairs arrive one at a time after
+    the runs ("queries_after_runs"), the FDTD answers each pair with one
+    source's share of a batched run of its wall set, and the readout pays
+    that share for each rejected pair. The committee's
     disagreement is scaled to a predicted error by the `calib_q` quantile of
     true error / disagreement over the validation receivers. Reports
     errors, the fraction within the bound, IRs/s of each path and the gain
@@ -535,11 +535,14 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     fdtd_alone_s = float(np.sum(fd_s))  # one batched run per wall set answers every query pair
     irs_fdtd = n_pairs / fdtd_alone_s
     irs_sur = n_pairs / (t_pred + t_fallback)
-    # query positions arriving after the runs: one batched run per position
-    t_run = float(np.mean(fd_s))
-    positions_rejected = int((~accept).any(axis=1).sum())  # [n_sets, n_query] positions with a rejected source
-    irs_fdtd_after = n_pairs / (n_sets * n_query * t_run)
-    irs_sur_after = n_pairs / (t_pred + positions_rejected * t_run)
+    # query pairs arriving one at a time after the runs: the FDTD answers each
+    # with one source's share of a batched run (cheaper than a plain
+    # single-source run, so the comparison favours the FDTD); the readout
+    # pays that only for its rejected pairs
+    t_pair = float(np.mean(fd_s)) / n_src
+    rejected = int((~accept).sum())
+    irs_fdtd_after = 1.0 / t_pair
+    irs_sur_after = n_pairs / (t_pred + rejected * t_pair)
     return {
         "wall_sets": n_sets, "sources_per_set": n_src, "grid_receivers": ng, "grid_spacing_m": d["grid_h"],
         "query_pairs": n_pairs, "validation_pairs": n_sets * n_src * n_val, "features": n_feat,
@@ -556,7 +559,7 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
         "irs_per_s": {"readout_only": n_pairs / t_pred, "readout_with_fallback": irs_sur,
                       "batched_fdtd": irs_fdtd, "plain_fdtd": (16 / t_plain) if t_plain else None},
         "gain_over_fdtd": irs_sur / irs_fdtd, "bound": bound, "calibration_quantile": calib_q,
-        "queries_after_runs": {"fallback_runs": positions_rejected, "positions": n_sets * n_query,
+        "queries_after_runs": {"fallback_runs": rejected, "fdtd_s_per_pair": t_pair,
                                "irs_per_s": {"readout_with_fallback": irs_sur_after, "fdtd": irs_fdtd_after},
                                "gain_over_fdtd": irs_sur_after / irs_fdtd_after},
     }

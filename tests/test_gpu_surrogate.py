@@ -158,10 +158,11 @@ def test_field_readout_gain_over_fdtd(pkg):
     positions the generating run did not train on: the fraction of pairs
     within 1 % relative L2, the IRs/s with FDTD fallback for the pairs whose
     predicted error exceeds 1 %, and the gain over the FDTD alone. Where the
-    query positions arrive after the runs, the FDTD needs one run per new
-    position and the readout gains; where every position is known before
-    the runs, one batched FDTD run answers them all and the readout with
-    fallback runs cannot beat it (that gain is printed, not asserted)."""
+    query pairs arrive one at a time after the runs, the FDTD pays one
+    source's share of a batched run per pair and the readout only for its
+    rejected pairs; where every position is known before the runs, one
+    batched FDTD run answers them all and the readout with its fallback runs
+    cannot beat it (that gain is printed, and bounded below only)."""
     import ancfield_b200.surrogate_workflow as SW
     r = SW.run_field_readout(pkg, n_sets=1, n_src=4, n_query=64, n_val=64, plain=False)
     print({k: r[k] for k in ("query_rel_l2", "within_bound", "accepted", "accepted_but_over_bound",
@@ -169,5 +170,5 @@ def test_field_readout_gain_over_fdtd(pkg):
     assert r["within_bound"] >= 0.6
     # accepted pairs whose true error exceeds the bound: at most 3 %
     assert r["accepted_but_over_bound"] <= 0.03 * r["query_pairs"]
-    assert r["queries_after_runs"]["gain_over_fdtd"] > 1.0
+    assert r["queries_after_runs"]["gain_over_fdtd"] > 1.5
     assert r["gain_over_fdtd"] > 0.9
