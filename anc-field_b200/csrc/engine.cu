@@ -441,8 +441,11 @@ __device__ __forceinline__ void store4t(T* p, const float v[4], unsigned m, floa
 template <bool PSI, typename T>
 __device__ __forceinline__ void pml_p_unit(const StepArgs& a, int b, int x, int y, int z, long long g,
                                            float s_new, float ic, float io) {
+    // The mask gates only the stores and the flag: the loads below issue
+    // without waiting for it (every unit of a box lies in planes and rows
+    // 2..n-3, so x-1 .. x+4, y+-1 and z+-1 stay inside the level and field
+    // arrays even for a unit with no PML cell, whose results are dropped).
     const unsigned m = pml_mask4(a, x, y, z);
-    if (!m) return;
     const PmlDev& P = a.pml;
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
@@ -451,11 +454,12 @@ __device__ __forceinline__ void pml_p_unit(const StepArgs& a, int b, int x, int 
     const T* po = level_ptr<T>(a, buf_old(g)) + base;
     T* pn = level_ptr<T>(a, buf_new(g)) + base;
     const int lv = pml_level(a, g);
-    // x+4 is read only for the unit's last cell, x-1 only for its first
-    const bool hi = (m & 8u) != 0;
+    // x+4 is read only where it lies in the row (the unit's last cell can be
+    // a PML cell only then)
+    const bool hi = x + 4 < a.g.pitch;
     float c[5], ym4[5], yp4[5], zm4[5], zp4[5], o[5];
     row5t(pc + i, c, ic, hi);
-    const float xm = (m & 1u) ? fldg(pc + i - 1, ic) : 0.0f;
+    const float xm = x >= 1 ? fldg(pc + i - 1, ic) : 0.0f;
     row5t(pc + i - pitch, ym4, ic, false);
     row5t(pc + i + pitch, yp4, ic, false);
     row5t(pc + i - plane, zm4, ic, false);
@@ -564,8 +568,8 @@ __device__ __forceinline__ void pml_p_unit(const StepArgs& a, int b, int x, int 
 template <int AX, bool PSI, typename T>
 __device__ __forceinline__ void pml_aux_unit(const StepArgs& a, int b, int x, int y, int z, long long g,
                                              float in_, float ic) {
+    // loads issue without waiting for the mask, as in pml_p_unit
     const unsigned m = pml_mask4(a, x, y, z);
-    if (!m) return;
     const PmlDev& P = a.pml;
     const size_t base = (size_t)b * a.g.vol;
     const int64_t pitch = a.g.pitch, plane = a.g.plane;
@@ -573,7 +577,7 @@ __device__ __forceinline__ void pml_aux_unit(const StepArgs& a, int b, int x, in
     const T* pn = level_ptr<T>(a, buf_new(g)) + base + i;
     const T* pc = level_ptr<T>(a, buf_cur(g)) + base + i;
     const int lv = pml_level(a, g);
-    const bool hi = (m & 8u) != 0;  // x+4 is read only for the unit's last cell
+    const bool hi = x + 4 < a.g.pitch;  // x+4 is read only where it lies in the row
     float n00[5], n01[5], n10[5], n11[5], m00[5], m01[5], m10[5], m11[5];
     row5t(pn, n00, in_, hi);
     row5t(pn + plane, n01, in_, hi);
