@@ -900,8 +900,10 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
     // FP16: the level scales of the current member, loaded again only when
     // a work item of another member comes (items of one member are
     // consecutive in the list), so the L2 load is off most items' path
+    // (kept as the three factors the update uses: s_new / s_cur, s_cur /
+    // s_old and 1 / s_cur)
     int sc_b = -1;
-    StepScales sc_cached{};
+    float sc_rc = 1.0f, sc_ro = 1.0f, sc_ic = 1.0f;
     uint32_t k = 0;
     while (true) {
         if (!mbar_wait(&full[k % F_STAGES], (k / F_STAGES) & 1)) {
@@ -972,11 +974,13 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
             // only z+1, y+-1 and p^{n-1}. The update runs on stored values
             // of level g-1 (scale s_cur) and is rescaled once at the end.
             if (it.b != sc_b) {
-                sc_cached = step_scales(a.f16, it.b, g);
+                const StepScales sc = step_scales(a.f16, it.b, g);
+                sc_rc = sc.s_new * sc.inv_cur;
+                sc_ro = sc.s_cur * sc.inv_old;
+                sc_ic = sc.inv_cur;
                 sc_b = it.b;
             }
-            const StepScales sc = sc_cached;
-            const float rc = sc.s_new * sc.inv_cur, ro = sc.s_cur * sc.inv_old;
+            const float rc = sc_rc, ro = sc_ro;
             uint32_t vmask[4];
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -1037,7 +1041,13 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
                         s = s + ym[m];
                         s = s + zp[m];
                         s = s + zm[m];
-                        v2[h] = (c[m] + ((c[m] - o[m] * ro) + L2 * (s - 6.0f * c[m]))) * rc;
+                        // c and o are decoded binary16 values (at most 11
+                        // significant bits) and ro a power of two, so o * ro
+                        // and 6 * c are exact: the fused forms round once,
+                        // as the separate product and difference do
+                        const float inc = __fmaf_rn(-o[m], ro, c[m]);   // c - o * ro
+                        const float lap = __fmaf_rn(-6.0f, c[m], s);    // s - 6 c
+                        v2[h] = (c[m] + (inc + L2 * lap)) * rc;
                     }
                     const __half2 hv = __floats2half2_rn(v2[0], v2[1]);
                     outw[w] = *reinterpret_cast<const uint32_t*>(&hv);
@@ -1075,7 +1085,7 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
             // together with the others below
             const uint32_t gmax = __reduce_max_sync(0xffffffffu, max(amax & 0xffffu, amax >> 16));
             if (lane == 0 && gmax) {
-                const float mv = __half2float(__ushort_as_half((unsigned short)gmax)) * sc.inv_cur;
+                const float mv = __half2float(__ushort_as_half((unsigned short)gmax)) * sc_ic;
                 atomicMax(a.f16.mx + (size_t)it.b * 5 + max_slot(g - 1), __float_as_uint(mv));
             }
             // a stored binary16 infinity or NaN (magnitude bits >= 0x7c00)
