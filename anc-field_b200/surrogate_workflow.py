@@ -445,6 +445,37 @@ def field_data(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, seed=21, grid_h=GRI
             "grid_h": grid_h, "seed": seed}
 
 
+def readout_accounting(accept, t_pred, fd_s, t_plain=None):
+    """IRs/s of the readout with its FDTD fallback against the FDTD alone.
+    accept [n_sets, n_src, n_query]: pairs whose predicted error is within
+    the bound; t_pred: seconds of the readout's predictions for every pair;
+    fd_s: seconds of the batched FDTD run of each wall set (all its
+    sources); t_plain: seconds of one plain single-source run (else one
+    source's share of a batched run).
+    Queries known before the runs: the FDTD answers every pair with one
+    batched run per wall set; the readout falls back to one single-source
+    run per (wall set, source) with a rejected pair.
+    Query pairs arriving one at a time after the runs: the FDTD answers each
+    with one source's share of a batched run (measured no slower than a
+    plain single-source run); the readout pays that share for each rejected
+    pair only."""
+    accept = np.asarray(accept, bool)
+    n_sets, n_src, n_query = accept.shape
+    n_pairs = n_sets * n_src * n_query
+    t_share = float(np.mean(fd_s)) / n_src
+    t_single = t_plain if t_plain is not None else t_share
+    runs_needed = int((~accept).any(axis=2).sum())
+    rejected = int((~accept).sum())
+    irs_fdtd = n_pairs / float(np.sum(fd_s))
+    irs_readout = n_pairs / (t_pred + runs_needed * t_single)
+    irs_fdtd_after = 1.0 / t_share
+    irs_readout_after = n_pairs / (t_pred + rejected * t_share)
+    return {"query_pairs": n_pairs, "fallback_runs": runs_needed, "rejected_pairs": rejected,
+            "irs_fdtd": irs_fdtd, "irs_readout": irs_readout, "gain": irs_readout / irs_fdtd,
+            "t_pair": t_share, "irs_fdtd_after": irs_fdtd_after, "irs_readout_after": irs_readout_after,
+            "gain_after": irs_readout_after / irs_fdtd_after}
+
+
 def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, seed=21, n_feat=4096,
                       sigma=2.0, ridge=1e-4, grid_h=GRID_H, plain=True, data=None, near=True, calib_q=0.8):
     """The learned readout against the FDTD for receiver positions that the
@@ -526,24 +557,15 @@ def run_field_readout(pkg, n_sets=2, n_src=8, n_query=96, n_val=96, bound=0.01, 
     far = dist >= 0.5
     pe = calib * dq
     accept = pe <= bound
-    runs_needed = int((~accept).any(axis=2).sum())
     t_plain = None
     if plain:
         _, t_plain = plain_irs(pkg, d["gsets"][0], d["srcs"][0][0], q_cells[:16])
-    t_single = t_plain if t_plain is not None else float(np.mean(fd_s)) / n_src
-    n_pairs = n_sets * n_src * n_query
-    t_fallback = runs_needed * t_single
-    fdtd_alone_s = float(np.sum(fd_s))  # one batched run per wall set answers every query pair
-    irs_fdtd = n_pairs / fdtd_alone_s
-    irs_sur = n_pairs / (t_pred + t_fallback)
-    # query pairs arriving one at a time after the runs: the FDTD answers each
-    # with one source's share of a batched run (cheaper than a plain
-    # single-source run, so the comparison favours the FDTD); the readout
-    # pays that only for its rejected pairs
-    t_pair = float(np.mean(fd_s)) / n_src
-    rejected = int((~accept).sum())
-    irs_fdtd_after = 1.0 / t_pair
-    irs_sur_after = n_pairs / (t_pred + rejected * t_pair)
+    acc = readout_accounting(accept, t_pred, fd_s, t_plain)
+    n_pairs = acc["query_pairs"]
+    runs_needed, rejected = acc["fallback_runs"], acc["rejected_pairs"]
+    irs_fdtd, irs_sur = acc["irs_fdtd"], acc["irs_readout"]
+    irs_fdtd_after, irs_sur_after = acc["irs_fdtd_after"], acc["irs_readout_after"]
+    t_pair = acc["t_pair"]
     return {
         "wall_sets": n_sets, "sources_per_set": n_src, "grid_receivers": ng, "grid_spacing_m": d["grid_h"],
         "query_pairs": n_pairs, "validation_pairs": n_sets * n_src * n_val, "features": n_feat,
