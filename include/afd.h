@@ -333,7 +333,9 @@ typedef struct afd_plan {
  * for this simulation (no counterpart in the reference, whose kernels have
  * one launch shape: clh-kernel.hpp:163-183). NULL gives the plan back to the
  * autotuner, which tries its candidates again. Every plan gives the same
- * results bit for bit. */
+ * receivers bit for bit, and the same pressure at every cell an air cell
+ * reads; the 32x32 tile leaves out work items whose region holds no air, so
+ * solid cells more than one cell from air keep older values there. */
 int afd_set_plan(afd_sim* s, const afd_plan* plan);
 
 /* z-slab domain decomposition (no counterpart in the reference, which runs
