@@ -750,11 +750,13 @@ def e2e_leg(sim, cfg, K, interior, world, metric):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
 # dominant kernel, from one single-pass ncu capture of that kernel on the
-# full-size workload under the forced plan of the key (`--plan 64x16:8` or
-# `--plan 128x8:8`), keyed by grid, storage, tile and tail warps; the line
+# full-size workload under the forced plan of the key (`--plan 64x16:8`,
+# `--plan 128x8:8`, `--storage fp16 --plan 64x32:16`), keyed by grid,
+# storage, tile and tail warps; the line
 # reports it with traffic_source "ncu capture".
 MEASURED_TRAFFIC = {((512, 384, 320), "fp32", (64, 16), False): ("interior_stream", 740.42e6),
-                    ((512, 384, 320), "fp32", (128, 8), False): ("interior_stream", 724.12e6)}
+                    ((512, 384, 320), "fp32", (128, 8), False): ("interior_stream", 724.12e6),
+                    ((512, 384, 320), "fp16", (64, 32), False): ("interior_stream", 353.99e6)}
 
 
 def roofline_leg(make_sim, K, interior, bytes_per_cell=12.0, traffic_key=None, plan=None, step_parts=None):
