@@ -1,7 +1,7 @@
 // Learned impulse-response surrogate: a Fourier-feature MLP trained and
 // evaluated with hand-written tcgen05 BF16 GEMMs (FP32 accumulation in
 // TMEM) on sm_100a. No counterpart in the reference; the FDTD engine of
-// this library generates its training data and judges its error.
+// this library generates its training data and measures its error.
 //
 // Network: x (n_in values in [0, 1]) -> [sin(2 pi x B), cos(2 pi x B)]
 // (B: n_in x n_freq, N(0, sigma^2)) -> (n_layers - 1) x [Linear + ReLU] ->
