@@ -944,6 +944,7 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
                 const float4 zp = *reinterpret_cast<const float4*>(Pp + s0);
                 const float4 o = *reinterpret_cast<const float4*>(O + cy * TL::W + cx);
                 __syncwarp();
+                fence_async_smem();
                 if (lane == 0) mbar_arrive(&empty[km % F_STAGES]);  // plane z-1 no longer read
                 float4 v;
                 v.x = slf_update(L2, CI, c.y, xm, yp.x, ym.x, zp.x, zm.x, c.x, o.x);
@@ -1001,6 +1002,7 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
                 cvt8(wb, rb);
             }
             __syncwarp();
+            fence_async_smem();
             if (lane == 0) mbar_arrive(&empty[k % F_STAGES]);  // plane z0-1 now in registers
             uint32_t amax = 0, omax = 0;
             // one plane: zm, c, zp rotate through ra, rb, rcv
@@ -1019,6 +1021,7 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
                 const uint4 ow = *reinterpret_cast<const uint4*>(O + so);
                 const float xm = __half2float(P0[s0 - 1]), xp = __half2float(P0[s0 + 8]);
                 __syncwarp();
+                fence_async_smem();
                 if (lane == 0) mbar_arrive(&empty[kc % F_STAGES]);  // plane z read
                 amax = __vmaxu2(amax, __vmaxu2(__vmaxu2(cw.x & vmask[0], cw.y & vmask[1]),
                                                __vmaxu2(cw.z & vmask[2], cw.w & vmask[3])));
@@ -1093,12 +1096,14 @@ __global__ void __launch_bounds__(TAIL ? F_THREADS + 32 * kTailWarps : F_THREADS
             const uint32_t om = max(omax & 0xffffu, omax >> 16);
             bad = om >= 0x7c00u;
             __syncwarp();
+            fence_async_smem();
             if (lane == 0) mbar_arrive(&empty[(k + planes + 1) % F_STAGES]);
             if (__any_sync(0xffffffffu, bad && yok && x <= a.g.nx - 2) && lane == 0) atomicOr(a.flag, 1);
             k += (uint32_t)planes + 2;
             continue;
         }
         __syncwarp();
+        fence_async_smem();
         if (lane == 0) {
             mbar_arrive(&empty[(k + planes) % F_STAGES]);
             mbar_arrive(&empty[(k + planes + 1) % F_STAGES]);

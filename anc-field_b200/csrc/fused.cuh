@@ -81,6 +81,13 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
+// A consumer's release of a stage: its shared-memory reads of the stage go
+// through the generic proxy, the TMA load that refills the stage once the
+// producer sees the release writes through the async proxy. The proxy fence
+// orders this thread's reads before those writes; without it a refill could
+// land before a read of the old plane completed (seen as one-unit differences
+// between runs of the FP16 kernel, whose consumers release a plane early).
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
