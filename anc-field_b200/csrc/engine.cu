@@ -1130,11 +1130,6 @@ static StreamShape stream_shape_t() {
                        (const void*)k_stream<T, S, TAIL>};
 }
 static bool shape_valid(bool f16, int S) { return S >= 0 && S < kTileShapes && !(f16 && S == 1); }
-// FP16 storage with the 64x32 tile (shape 2): z-chunks of at least 16 planes.
-// With 8-plane chunks, runs of the 16-member batch differed from the serial
-// run before the consumers fenced their stage releases (fence_async_smem);
-// the bound dates from then and costs nothing (the tuner keeps 16 or 32).
-constexpr int kF16TallMinDz = 16;
 // tail: the instance with tail warps (FP32 storage only)
 static StreamShape stream_shape(bool f16, int S, bool tail = false) {
     if (f16) return S == 2 ? stream_shape_t<__half, 2>() : stream_shape_t<__half, 0>();
@@ -1522,7 +1517,6 @@ struct Engine::Impl {
         }
         auto add = [&](int ps, int d, bool bs, int sh, bool tl) {
             if (ps < 1 || d < 8) return;
-            if (f16() && sh == 2 && d < kF16TallMinDz) return;
             for (const Plan& q : tune_cands)
                 if (q.per_sm == ps && q.dz == d && q.beside == bs && q.shape == sh && q.tail == tl) return;
             tune_cands.push_back(Plan{ps, d, bs, sh, tl});
@@ -1838,7 +1832,6 @@ void Engine::Impl::build_fused() {
     F.tail = f_tail.ptr;
     const int64_t tiles = (int64_t)tiles_x * tiles_y * prm.batch;
     int dz = chunk_rule(tiles, nz, resident);
-    if (f16() && plan.shape == 2) dz = std::max(dz, kF16TallMinDz);
     rule_dz = dz;
     if (plan.dz > 0) dz = plan.dz;
     F.dz = dz;
@@ -2613,10 +2606,6 @@ void Engine::set_plan(const afd_plan* p) {
         if (shape < 0)
             throw Error(AFD_ERR_ARG, D.f16() ? "unsupported streaming tile (FP16 storage: 128x16 or 64x32)"
                                              : "unsupported streaming tile (64x16, 128x8 or 32x32)");
-        if (p->beside && D.f16())
-            throw Error(AFD_ERR_ARG, "beside plans are FP32-only");
-        if (D.f16() && shape == 2 && p->dz > 0 && p->dz < kF16TallMinDz)
-            throw Error(AFD_ERR_ARG, "FP16 storage with the 64x32 tile needs z-chunks of 16 planes or more");
         if (p->per_sm < 0 || p->per_sm > 32) throw Error(AFD_ERR_ARG, "per_sm out of range (0..32)");
         if (p->dz < 0 || p->dz > 1024) throw Error(AFD_ERR_ARG, "dz out of range (0..1024)");
     }

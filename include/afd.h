@@ -316,11 +316,8 @@ int afd_set_stream(afd_sim* s, void* stream);
  * the default: the 64x16 tile, as many resident blocks per SM as fit, the
  * z-chunk depth rule. beside = 1 runs the boundary and PML pressure kernels
  * beside the streaming kernel, which then skips their cells (FIXED scheme
- * with CUDA graphs; FP32 storage only: AFD_ERR_ARG with FP16 storage; ignored
- * elsewhere). With FP16 storage the 64x32 tile takes z-chunks of 16 planes or
- * more (AFD_ERR_ARG for 1..15; the depth rule is raised to 16 for it). The
- * autotuner tries neither the beside nor the tail order (both measured
- * slower). */
+ * with CUDA graphs; ignored elsewhere). The autotuner tries neither the
+ * beside nor the tail order (both measured slower). */
 typedef struct afd_plan {
     int32_t tile_x, tile_y;  /* streaming tile in cells: 64x16, 128x8 or 32x32 (FP16 storage doubles x) */
     int32_t per_sm;          /* resident streaming blocks per SM */
